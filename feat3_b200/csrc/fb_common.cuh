@@ -1,0 +1,94 @@
+// Shared device/host helpers of the feat3_b200 sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include <cmath>
+
+#include "../../include/feat3_b200.h"
+
+namespace fb {
+
+constexpr int kSMs = 148;            // B200: 2 dies x 74 SMs
+constexpr int kWarp = 32;
+constexpr int kRedBlocks = 4 * kSMs; // reduction grid: 4 resident CTAs per SM
+constexpr int kRedThreads = 256;
+
+// map a CUDA error onto the C-ABI status
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? FB_OK : FB_ERR_CUDA; }
+#define FB_CHECK_LAUNCH() do { cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
+#define FB_TRY(x) do { int _s = (x); if (_s != FB_OK) return _s; } while (0)
+#define FB_CUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
+
+inline unsigned grid_for(uint64_t n, int threads, int per_thread = 1) {
+  uint64_t g = (n + uint64_t(threads) * per_thread - 1) / (uint64_t(threads) * per_thread);
+  if (g < 1) g = 1;
+  if (g > 0x7fffffffull) g = 0x7fffffffull;
+  return unsigned(g);
+}
+
+template<typename T> __host__ __device__ constexpr T eps_of();
+template<> __host__ __device__ constexpr double eps_of<double>() { return 2.220446049250313e-16; }
+template<> __host__ __device__ constexpr float eps_of<float>() { return 1.1920928955078125e-07f; }
+
+// ---------------------------------------------------------------------------------------
+// deterministic two-stage reduction: every CTA writes one partial, the last CTA to finish
+// sums the partials in index order and writes the scalar. `ws` = [partials (gridDim)],
+// `counter` = one u32 that must be 0 before the launch; the last CTA resets it to 0.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template<int THREADS>
+__device__ __forceinline__ double block_sum(double v, double* sh /* THREADS/32 */) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = (lane < THREADS / 32) ? sh[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;  // valid in thread 0
+}
+
+// Finish a reduction: thread 0 of every CTA passes its CTA partial. Returns true in the one
+// thread (of the last CTA) that wrote `*out` (the final sum, optionally transformed).
+// The partials buffer and counter live in `ws`/`counter`.
+template<int THREADS>
+__device__ __forceinline__ bool reduce_finish(double blk, double* ws, unsigned* counter, double* out,
+                                              double* sh, bool take_sqrt = false) {
+  __shared__ bool am_last;
+  if (threadIdx.x == 0) {
+    ws[blockIdx.x] = blk;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double v = 0.0;
+  // fixed order: thread t sums partials t, t+THREADS, ...
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += THREADS) v += ((volatile double*)ws)[i];
+  v = block_sum<THREADS>(v, sh);
+  if (threadIdx.x == 0) {
+    *out = take_sqrt ? sqrt(v) : v;
+    *counter = 0u;
+  }
+  return threadIdx.x == 0;
+}
+
+// per-device library workspace for the stand-alone reductions of the operator C-ABI
+struct Workspace {
+  double* partials = nullptr;   // kRedBlocks doubles
+  unsigned* counter = nullptr;  // one counter per concurrent reduction slot
+  double* result = nullptr;     // device scalar used by the *_sync host-returning variants
+  double* host_result = nullptr;
+};
+int workspace_get(Workspace** ws);
+
+}  // namespace fb

@@ -1,0 +1,904 @@
+// Native multigrid driver: device hierarchy (SELL-C-sigma level matrices, CSR transfers,
+// Dirichlet bit masks), the fused V-cycle, PCG / Richardson outer solvers in FP64 and in
+// mixed precision (FP64 outer defect and update around an FP32 V-cycle with FP32 or FP16
+// matrix values), structured Q1/Q2 device assembly, and the adjoint gradient.
+//
+// The operator sequence is the reference's (kernel/solver/multigrid.hpp:1268-2000,
+// pcg.hpp:188-287, richardson.hpp:160-226, jacobi_precond.hpp:137-165); fusion only merges
+// operations that the reference performs back to back on the same rows:
+//   * pre-smoothing from a zero guess: step 1 is an element-wise Jacobi update (fused into
+//     the restriction that produced the level's right-hand side), steps 2..nu are fused
+//     defect+update SpMVs; the smoother's final defect equals the defect multigrid
+//     recomputes afterwards, so it is computed once;
+//   * post-smoothing: Richardson on the correction from zero with rhs d = b - A s0 equals
+//     Jacobi on the level system started at s0 (same iterates in exact arithmetic), so each
+//     step is one fused SpMV and the discarded last smoother defect is never formed;
+//   * the smoother's initial-norm test (skip on a non-finite or <= eps^2 defect) is kept:
+//     the norm is reduced inside the kernel that produces the defect and read by the next.
+#include "fb_mg_internal.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+namespace fb {
+
+static int occupancy_grid(const void* fn, uint64_t work_warps) {
+  // blocks of 256 threads; at most the resident capacity of all SMs
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, 256, 0) != cudaSuccess || bps < 1) bps = 4;
+  uint64_t need = (work_warps + 7) / 8;
+  uint64_t cap = uint64_t(bps) * kSMs;
+  uint64_t g = need < cap ? need : cap;
+  return int(g < 1 ? 1 : g);
+}
+
+// ------------------------------------------------------------------ launch helpers
+template<typename VT, typename XT, typename AT, typename Epi>
+static int launch_sell(fb_mg* m, const DevSell& A, int prec, const XT* x, const Epi& epi, double* red_out) {
+  auto fn = k_sell<VT, XT, AT, Epi, 8>;
+  const int grid = occupancy_grid((const void*)fn, A.nchunks);
+  fn<<<grid, 256, 0, m->stream>>>(A.view(prec), x, epi, m->ws, m->counter, red_out);
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
+template<typename VT, typename XT, typename AT, typename Epi>
+static int launch_csr(fb_mg* m, const DevCsr& A, bool f32, const XT* x, const Epi& epi, double* red_out) {
+  const double avg = A.rows ? double(A.nnz) / double(A.rows) : 0.0;
+  if (avg <= 4.0) {
+    auto fn = k_csr_epi<VT, XT, AT, Epi, 4>;
+    fn<<<occupancy_grid((const void*)fn, (uint64_t(A.rows) * 4 + 31) / 32), 256, 0, m->stream>>>(A.view(f32), x, epi, m->ws, m->counter, red_out);
+  } else if (avg <= 12.0) {
+    auto fn = k_csr_epi<VT, XT, AT, Epi, 8>;
+    fn<<<occupancy_grid((const void*)fn, (uint64_t(A.rows) * 8 + 31) / 32), 256, 0, m->stream>>>(A.view(f32), x, epi, m->ws, m->counter, red_out);
+  } else {
+    auto fn = k_csr_epi<VT, XT, AT, Epi, 16>;
+    fn<<<occupancy_grid((const void*)fn, (uint64_t(A.rows) * 16 + 31) / 32), 256, 0, m->stream>>>(A.view(f32), x, epi, m->ws, m->counter, red_out);
+  }
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
+// ------------------------------------------------------------------ small kernels
+// s1 = skip ? 0 : omega * filter_cor(invd o b)   (first pre-smoothing step from zero)
+template<typename T>
+__global__ void k_jacobi0(T* out, const T* __restrict__ b, const T* __restrict__ invd, const uint32_t* mask,
+                          const double* skip_src, T omega, uint32_t n) {
+  const bool skip = smoother_skip<T>(skip_src);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = (skip || masked(mask, i)) ? T(0) : omega * (invd[i] * b[i]);
+}
+
+// post-smoothing with nu == 1: restore the prolongated iterate when the smoother skipped
+template<typename T>
+__global__ void k_skip_fix(T* out, const T* __restrict__ s0, const double* skip_src, uint32_t n) {
+  if (!smoother_skip<T>(skip_src)) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = s0[i];
+}
+
+// dense coarse solve: x = Cinv b (Cinv = inverse of the filtered coarse matrix, zero
+// Dirichlet rows/columns); one warp per row
+template<typename T>
+__global__ void k_dense_solve(T* x, const T* __restrict__ cinv, const T* __restrict__ b, uint32_t n) {
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  double s = 0.0;
+  for (uint32_t j = lane; j < n; j += 32) s += double(cinv[uint64_t(warp) * n + j]) * double(b[j]);
+  s = warp_sum(s);
+  if (lane == 0) x[warp] = T(s);
+}
+
+// coarse "none": x = filter_cor(b)
+template<typename T>
+__global__ void k_copy_masked(T* x, const T* __restrict__ b, const uint32_t* mask, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = masked(mask, i) ? T(0) : b[i];
+}
+
+// PCG update: alpha = gamma / qp; x += alpha p; r -= alpha q; ||r||^2 (+ FP32 copy of r)
+// (pcg.hpp:241-251 with the |alpha| < eps shortcut of dense_vector.hpp:891-895)
+template<bool LOW>
+__global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float* r32, const double* __restrict__ p,
+                                                    const double* __restrict__ q, const DevScalars* sc, uint32_t n,
+                                                    double* ws, unsigned* counter, double* rr_out) {
+  __shared__ double sh[8];
+  const double alpha = sc->gamma / sc->qp;
+  const bool upd = fabs(alpha) >= eps_of<double>();
+  double acc = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double ri = r[i];
+    if (upd) {
+      x[i] = alpha * p[i] + x[i];
+      ri = (-alpha) * q[i] + ri;
+      r[i] = ri;
+    }
+    if (LOW) r32[i] = float(ri);
+    acc += ri * ri;
+  }
+  const double blk = block_sum<256>(acc, sh);
+  reduce_finish<256>(blk, ws, counter, rr_out, sh, false);
+}
+
+// r . z with z in FP64 or FP32 (ConvertPrecond: z = double(z_inner))
+template<typename ZT>
+__global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, const ZT* __restrict__ z, uint32_t n,
+                                                double* ws, unsigned* counter, double* out) {
+  __shared__ double sh[8];
+  double acc = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc += r[i] * double(z[i]);
+  const double blk = block_sum<256>(acc, sh);
+  reduce_finish<256>(blk, ws, counter, out, sh, false);
+}
+
+// p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is done by the next kernel
+template<typename ZT>
+__global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+  const double beta = sc->rz / sc->gamma;
+  const bool upd = fabs(beta) >= eps_of<double>();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = upd ? beta * p[i] + double(z[i]) : double(z[i]);
+}
+
+__global__ void k_commit_gamma(DevScalars* sc) { sc->gamma = sc->rz; }
+__global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; }
+
+// Richardson outer: x = omega * z + x
+template<typename ZT>
+__global__ void k_rich_update(double* x, const ZT* __restrict__ z, double omega, uint32_t n) {
+  if (fabs(omega) < eps_of<double>()) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = omega * double(z[i]) + x[i];
+}
+
+template<typename T>
+__global__ void k_fill(T* x, T v, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = v;
+}
+
+__global__ void k_invdiag(double* invd64, float* invd32, const double* __restrict__ diag, double omega, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = omega / diag[i];
+    if (invd64) invd64[i] = v;
+    if (invd32) invd32[i] = float(omega) / float(diag[i]);
+  }
+}
+
+template<typename D, typename S>
+__global__ void k_cvt(D* d, const S* __restrict__ s, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) d[i] = D(s[i]);
+}
+
+__global__ void k_absmax(const double* __restrict__ v, uint64_t n, unsigned long long* out) {
+  double m = 0.0;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    m = fmax(m, fabs(v[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));  // non-negative doubles order as integers
+}
+
+__global__ void k_quant16(__half* d, const double* __restrict__ s, double inv, uint64_t n) {
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    d[i] = __double2half(s[i] * inv);
+}
+
+unsigned ew_grid(uint64_t n) {
+  unsigned g = grid_for(n, 256);
+  return g > 8u * kSMs ? 8u * kSMs : g;
+}
+
+// ------------------------------------------------------------------ V-cycle
+template<typename T> struct Prec;
+template<> struct Prec<double> {
+  static double* rhs(Level& l) { return l.rhs64; }
+  static double* x(Level& l) { return l.x64; }
+  static double* y(Level& l) { return l.y64; }
+  static double* def(Level& l) { return l.def64; }
+  static double* invd(Level& l) { return l.invd64; }
+};
+template<> struct Prec<float> {
+  static float* rhs(Level& l) { return l.rhs32; }
+  static float* x(Level& l) { return l.x32; }
+  static float* y(Level& l) { return l.y32; }
+  static float* def(Level& l) { return l.def32; }
+  static float* invd(Level& l) { return l.invd32; }
+};
+
+// dispatch a SELL launch on the value storage of the configured precision
+template<typename T, typename Epi>
+static int sell_T(fb_mg* m, const DevSell& A, const T* x, const Epi& epi, double* red) {
+  if (std::is_same<T, double>::value)
+    return launch_sell<double, double, double, Epi>(m, A, FB_PREC_F64, (const double*)x, epi, red);
+  if (m->cfg.precision == FB_PREC_F16)
+    return launch_sell<__half, float, float, Epi>(m, A, FB_PREC_F16, (const float*)x, epi, red);
+  return launch_sell<float, float, float, Epi>(m, A, FB_PREC_F32, (const float*)x, epi, red);
+}
+template<typename T, typename Epi>
+static int csr_T(fb_mg* m, const DevCsr& A, const T* x, const Epi& epi, double* red) {
+  if (std::is_same<T, double>::value)
+    return launch_csr<double, double, double, Epi>(m, A, false, (const double*)x, epi, red);
+  return launch_csr<float, float, float, Epi>(m, A, true, (const float*)x, epi, red);
+}
+
+// pre-smoothing from zero with rhs b on level l (Richardson(Jacobi), nu steps); `cur` holds
+// s1 on entry unless `need_s1`; returns the buffer with the smoothed iterate
+template<typename T>
+static int presmooth(fb_mg* m, int l, const T* b, const double* bnorm, bool need_s1, T** result) {
+  Level& L = m->L[l];
+  const T omega = T(m->cfg.omega_rich);
+  T* cur = Prec<T>::x(L);
+  T* oth = Prec<T>::y(L);
+  if (need_s1) {
+    k_jacobi0<T><<<ew_grid(L.n), 256, 0, m->stream>>>(cur, b, Prec<T>::invd(L), L.mask, bnorm, omega, L.n);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+  }
+  for (int it = 1; it < m->cfg.nu; ++it) {
+    EpiJacobi<T, false> e{cur, b, Prec<T>::invd(L), oth, nullptr, L.mask, bnorm, omega};
+    FB_TRY(sell_T<T>(m, L.A, cur, e, nullptr));
+    std::swap(cur, oth);
+  }
+  *result = cur;
+  return FB_OK;
+}
+
+template<typename T>
+static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** out_top) {
+  const int nl = (int)m->L.size();
+  const int nu = m->cfg.nu;
+  const T omega = T(m->cfg.omega_rich);
+  std::vector<T*> sol(nl, nullptr);
+  // ---- descent (multigrid.hpp:1711-1832)
+  for (int l = 0; l + 1 < nl; ++l) {
+    Level& L = m->L[l];
+    Level& C = m->L[l + 1];
+    const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
+    const double* bn = (l == 0) ? rhs_top_sumsq : &m->sc->lvl[2 * l];
+    const bool need_s1 = (l == 0) || nu < 2;
+    FB_TRY(presmooth<T>(m, l, b, bn, need_s1, &sol[l]));
+    EpiDefect<T, false, false> ed{Prec<T>::def(L), b, L.mask, nullptr};
+    FB_TRY(sell_T<T>(m, L.A, sol[l], ed, nullptr));
+    const bool coarsest_next = (l + 2 == nl);
+    T* s1 = nullptr;
+    if (nu >= 2 && (!coarsest_next || m->cfg.coarse == FB_COARSE_SMOOTHER)) s1 = Prec<T>::x(C);
+    EpiRestrict<T> er{Prec<T>::rhs(C), s1, Prec<T>::invd(C), C.mask, omega};
+    FB_TRY(csr_T<T>(m, L.R, Prec<T>::def(L), er, &m->sc->lvl[2 * (l + 1)]));
+  }
+  // ---- coarse grid (multigrid.hpp:1524-1587)
+  {
+    const int l = nl - 1;
+    Level& L = m->L[l];
+    const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
+    const double* bn = (l == 0) ? rhs_top_sumsq : &m->sc->lvl[2 * l];
+    switch (m->cfg.coarse) {
+      case FB_COARSE_DIRECT: {
+        const T* cinv = std::is_same<T, double>::value ? (const T*)m->cinv64 : (const T*)m->cinv32;
+        k_dense_solve<T><<<grid_for(uint64_t(L.n) * 32, 256), 256, 0, m->stream>>>(Prec<T>::x(L), cinv, b, L.n);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+      }
+      case FB_COARSE_SMOOTHER:
+        FB_TRY(presmooth<T>(m, l, b, bn, l == 0 || nu < 2, &sol[l]));
+        break;
+      case FB_COARSE_NONE:
+      default:
+        k_copy_masked<T><<<ew_grid(L.n), 256, 0, m->stream>>>(Prec<T>::x(L), b, L.mask, L.n);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+    }
+  }
+  // ---- ascent (multigrid.hpp:1843-2000)
+  for (int l = nl - 2; l >= 0; --l) {
+    Level& L = m->L[l];
+    const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
+    T* cur = sol[l];
+    T* oth = (cur == Prec<T>::x(L)) ? Prec<T>::y(L) : Prec<T>::x(L);
+    EpiProlong<T> ep{cur, L.mask};
+    FB_TRY(csr_T<T>(m, L.P, sol[l + 1], ep, nullptr));
+    T* s0 = cur;
+    double* dn = &m->sc->lvl[2 * l + 1];
+    for (int it = 0; it < nu; ++it) {
+      if (it == 0) {
+        EpiJacobi<T, true> e{cur, b, Prec<T>::invd(L), oth, nullptr, L.mask, nullptr, omega};
+        FB_TRY(sell_T<T>(m, L.A, cur, e, dn));
+        if (nu == 1) {
+          k_skip_fix<T><<<ew_grid(L.n), 256, 0, m->stream>>>(oth, s0, dn, L.n);
+          m->launches++;
+          FB_CHECK_LAUNCH();
+        }
+      } else {
+        EpiJacobi<T, false> e{cur, b, Prec<T>::invd(L), oth, s0, L.mask, dn, omega};
+        FB_TRY(sell_T<T>(m, L.A, cur, e, nullptr));
+      }
+      std::swap(cur, oth);
+    }
+    sol[l] = cur;
+  }
+  *out_top = sol[0];
+  return FB_OK;
+}
+
+// ------------------------------------------------------------------ stopping logic
+// IterativeSolver defaults and tests (kernel/solver/iterative.hpp:216-235, 490-505, 744-832)
+struct Stop {
+  double tol_rel, tol_abs, tol_abs_low = 0.0, div_rel, div_abs, def_init = 0.0;
+  int max_iter;
+  Stop(double tr, int mi) : tol_rel(tr), max_iter(mi) {
+    const double e = eps_of<double>();
+    tol_abs = 1.0 / (e * e); div_rel = 1.0 / e; div_abs = 1.0 / (e * e);
+  }
+  int initial(double d) {
+    def_init = d;
+    if (!std::isfinite(d)) return 3;
+    if (d <= eps_of<double>() * eps_of<double>()) return 2;
+    return 1;
+  }
+  int analyse(int it, double d) const {
+    if (!std::isfinite(d)) return 3;
+    if (d > div_abs || d > div_rel * def_init) return 4;
+    if ((d <= tol_abs) && ((d <= tol_rel * def_init) || (d <= tol_abs_low))) return 2;
+    if (it >= max_iter) return 5;
+    return 1;
+  }
+};
+
+// ------------------------------------------------------------------ solver bodies
+// outer defect r = filter_def(b - A x), ||r||^2, FP32 copy for the mixed V-cycle
+static int outer_defect(fb_mg* m) {
+  Level& L = m->L[0];
+  if (m->cfg.precision == FB_PREC_F64) {
+    EpiDefect<double, true, false> e{m->r, m->bb, L.mask, nullptr};
+    return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->xb, e, &m->sc->rr);
+  }
+  EpiDefect<double, true, true> e{m->r, m->bb, L.mask, m->r32};
+  return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->xb, e, &m->sc->rr);
+}
+
+// z-like output of the preconditioner (FP64 or FP32 buffer)
+static int precond(fb_mg* m, const void** z_out) {
+  if (m->cfg.precision == FB_PREC_F64) {
+    double* z = nullptr;
+    FB_TRY(vcycle<double>(m, m->r, &m->sc->rr, &z));
+    *z_out = z;
+  } else {
+    float* z = nullptr;
+    FB_TRY(vcycle<float>(m, m->r32, &m->sc->rr, &z));
+    *z_out = z;
+  }
+  return FB_OK;
+}
+
+// one outer iteration after a successful stopping test; ends with ||r||^2 copied to the host
+static int body(fb_mg* m) {
+  const uint32_t n = m->L[0].n;
+  const bool low = m->cfg.precision != FB_PREC_F64;
+  const void* z = nullptr;
+  FB_TRY(precond(m, &z));
+  if (m->cfg.outer == FB_OUTER_PCG) {
+    // gamma' = r . z ; p = z + beta p ; q = A p ; x, r update
+    if (low) k_dot_rz<float><<<occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz);
+    else     k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const double*)z, n, m->ws, m->counter, &m->sc->rz);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    if (low) k_pcg_dir<float><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const float*)z, m->sc, n);
+    else     k_pcg_dir<double><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const double*)z, m->sc, n);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    k_commit_gamma<<<1, 1, 0, m->stream>>>(m->sc);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
+    FB_TRY((launch_sell<double, double, double>(m, m->L[0].A, FB_PREC_F64, (const double*)m->p, eq, &m->sc->qp)));
+    if (low) k_pcg_update<true><<<occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
+    else     k_pcg_update<false><<<occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+  } else {
+    if (low) k_rich_update<float><<<ew_grid(n), 256, 0, m->stream>>>(m->xb, (const float*)z, m->cfg.omega_outer, n);
+    else     k_rich_update<double><<<ew_grid(n), 256, 0, m->stream>>>(m->xb, (const double*)z, m->cfg.omega_outer, n);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    FB_TRY(outer_defect(m));
+  }
+  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  return FB_OK;
+}
+
+static int run_body(fb_mg* m) {
+  if (!m->cfg.use_graphs) return body(m);
+  const int key = m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
+  if (!m->g_body || m->g_body_key != key) {
+    if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; }
+    cudaGraph_t g = nullptr;
+    FB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    const int before = m->launches;
+    int st = body(m);
+    cudaError_t e = cudaStreamEndCapture(m->stream, &g);
+    m->body_launches = m->launches - before;
+    m->launches = before;
+    if (st != FB_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return FB_ERR_CUDA;
+    e = cudaGraphInstantiate(&m->g_body, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { m->g_body = nullptr; return FB_ERR_CUDA; }
+    m->g_body_key = key;
+  }
+  m->launches += m->body_launches;
+  FB_CUDA(cudaGraphLaunch(m->g_body, m->stream));
+  return FB_OK;
+}
+
+static int ensure_vectors(fb_mg* m, int prec) {
+  if (m->prec_built == prec) return FB_OK;
+  const int nl = (int)m->L.size();
+  const bool low = prec != FB_PREC_F64;
+  for (int l = 0; l < nl; ++l) {
+    Level& L = m->L[l];
+    if (!low && !L.x64) {
+      if (l > 0) FB_TRY(dalloc(m, &L.rhs64, L.n));
+      FB_TRY(dalloc(m, &L.x64, L.n)); FB_TRY(dalloc(m, &L.y64, L.n)); FB_TRY(dalloc(m, &L.def64, L.n));
+    }
+    if (low && !L.x32) {
+      if (l > 0) FB_TRY(dalloc(m, &L.rhs32, L.n));
+      FB_TRY(dalloc(m, &L.x32, L.n)); FB_TRY(dalloc(m, &L.y32, L.n)); FB_TRY(dalloc(m, &L.def32, L.n));
+    }
+    if (!L.invd64) FB_TRY(dalloc(m, &L.invd64, L.n));
+    if (low && !L.invd32) FB_TRY(dalloc(m, &L.invd32, L.n));
+    k_invdiag<<<ew_grid(L.n), 256, 0, m->stream>>>(L.invd64, low ? L.invd32 : nullptr, L.diag, m->cfg.omega_jac, L.n);
+    FB_CHECK_LAUNCH();
+    if (low) {
+      if (!L.P.v32 && L.P.nnz) {
+        FB_TRY(dalloc(m, &L.P.v32, L.P.nnz)); FB_TRY(dalloc(m, &L.R.v32, L.R.nnz));
+        k_cvt<float, double><<<ew_grid(L.P.nnz), 256, 0, m->stream>>>(L.P.v32, L.P.v64, L.P.nnz);
+        k_cvt<float, double><<<ew_grid(L.R.nnz), 256, 0, m->stream>>>(L.R.v32, L.R.v64, L.R.nnz);
+        FB_CHECK_LAUNCH();
+      }
+      if (prec == FB_PREC_F32 && !L.A.v32) {
+        FB_TRY(dalloc(m, &L.A.v32, L.A.nent));
+        k_cvt<float, double><<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v32, L.A.v64, L.A.nent);
+        FB_CHECK_LAUNCH();
+      }
+      if (prec == FB_PREC_F16 && !L.A.v16) {
+        // per-level scale: the largest magnitude maps to 2^14 (headroom below 65504)
+        unsigned long long* dmax = nullptr;
+        FB_TRY(dalloc(m, &dmax, 1));
+        FB_CUDA(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), m->stream));
+        k_absmax<<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v64, L.A.nent, dmax);
+        FB_CHECK_LAUNCH();
+        unsigned long long hm = 0;
+        FB_CUDA(cudaMemcpyAsync(&hm, dmax, sizeof(hm), cudaMemcpyDeviceToHost, m->stream));
+        FB_CUDA(cudaStreamSynchronize(m->stream));
+        double amax;
+        std::memcpy(&amax, &hm, sizeof(double));
+        const double scale = amax > 0.0 ? amax / 16384.0 : 1.0;
+        L.A.scale16 = float(scale);
+        FB_TRY(dalloc(m, &L.A.v16, L.A.nent));
+        k_quant16<<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v16, L.A.v64, 1.0 / double(L.A.scale16), L.A.nent);
+        FB_CHECK_LAUNCH();
+      }
+    }
+  }
+  if (low && m->cinv64 && !m->cinv32) {
+    FB_TRY(dalloc(m, &m->cinv32, uint64_t(m->nc) * m->nc));
+    k_cvt<float, double><<<ew_grid(uint64_t(m->nc) * m->nc), 256, 0, m->stream>>>(m->cinv32, m->cinv64, uint64_t(m->nc) * m->nc);
+    FB_CHECK_LAUNCH();
+  }
+  const uint32_t n = m->L[0].n;
+  if (!m->r) {
+    FB_TRY(dalloc(m, &m->r, n)); FB_TRY(dalloc(m, &m->p, n)); FB_TRY(dalloc(m, &m->q, n));
+    FB_TRY(dalloc(m, &m->xb, n)); FB_TRY(dalloc(m, &m->bb, n));
+  }
+  if (low && !m->r32) FB_TRY(dalloc(m, &m->r32, n));
+  m->prec_built = prec;
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  return FB_OK;
+}
+
+// ------------------------------------------------------------------ setup: CSR -> SELL
+// SELL-C-sigma with C = 32: rows sorted by decreasing length inside windows of sigma rows
+int upload_sell(fb_mg* m, DevSell& S, const HostCsr& A, int sigma) {
+  const uint64_t n = A.rows;
+  if (n > 0xffffffffull) return FB_ERR_INVALID;
+  S.rows = uint32_t(n); S.cols = uint32_t(A.cols); S.nnz = A.rp[n];
+  S.nchunks = uint32_t((n + 31) / 32);
+  std::vector<uint32_t> perm(n);
+  std::iota(perm.begin(), perm.end(), 0u);
+  if (sigma > 1) {
+    for (uint64_t w = 0; w < n; w += sigma) {
+      const uint64_t e = std::min<uint64_t>(n, w + sigma);
+      std::stable_sort(perm.begin() + w, perm.begin() + e, [&](uint32_t a, uint32_t b) {
+        return (A.rp[a + 1] - A.rp[a]) > (A.rp[b + 1] - A.rp[b]);
+      });
+    }
+  }
+  std::vector<uint32_t> cs(S.nchunks + 1, 0), cl(S.nchunks, 0);
+  for (uint32_t c = 0; c < S.nchunks; ++c) {
+    uint32_t mx = 0;
+    for (uint32_t t = 0; t < 32; ++t) {
+      const uint64_t sr = uint64_t(c) * 32 + t;
+      if (sr < n) mx = std::max<uint32_t>(mx, uint32_t(A.rp[perm[sr] + 1] - A.rp[perm[sr]]));
+    }
+    cl[c] = mx;
+    const uint64_t nx = uint64_t(cs[c]) + uint64_t(mx) * 32;
+    if (nx > 0xffffffffull) return FB_ERR_INVALID;
+    cs[c + 1] = uint32_t(nx);
+  }
+  S.nent = cs[S.nchunks];
+  std::vector<uint32_t> col(S.nent, 0);
+  std::vector<double> val(S.nent, 0.0);
+  for (uint64_t sr = 0; sr < n; ++sr) {
+    const uint32_t row = perm[sr];
+    const uint32_t c = uint32_t(sr / 32), t = uint32_t(sr % 32);
+    uint32_t j = 0;
+    for (uint64_t k = A.rp[row]; k < A.rp[row + 1]; ++k, ++j) {
+      col[cs[c] + uint64_t(j) * 32 + t] = A.ci[k];
+      val[cs[c] + uint64_t(j) * 32 + t] = A.va[k];
+    }
+    // padding: column of the row itself (keeps x loads in the row's neighbourhood), value 0
+    for (; j < cl[c]; ++j) col[cs[c] + uint64_t(j) * 32 + t] = row < A.cols ? row : 0;
+  }
+  FB_TRY(dupload(m, &S.cs, cs.data(), cs.size()));
+  FB_TRY(dupload(m, &S.cl, cl.data(), cl.size()));
+  FB_TRY(dupload(m, &S.col, col.data(), col.size()));
+  FB_TRY(dupload(m, &S.v64, val.data(), val.size()));
+  {
+    std::vector<uint32_t> rl(n);
+    for (uint64_t i = 0; i < n; ++i) rl[i] = uint32_t(A.rp[i + 1] - A.rp[i]);
+    FB_TRY(dupload(m, &S.rl, rl.data(), rl.size()));
+  }
+  if (sigma > 1) FB_TRY(dupload(m, &S.perm, perm.data(), perm.size()));
+  return FB_OK;
+}
+
+int upload_csr(fb_mg* m, DevCsr& D, const HostCsr& A) {
+  if (A.rows > 0xffffffffull || A.rp[A.rows] > 0xffffffffull) return FB_ERR_INVALID;
+  D.rows = uint32_t(A.rows); D.cols = uint32_t(A.cols); D.nnz = A.rp[A.rows];
+  std::vector<uint32_t> rp(A.rp.begin(), A.rp.end());
+  FB_TRY(dupload(m, &D.rp, rp.data(), rp.size()));
+  FB_TRY(dupload(m, &D.col, A.ci.data(), A.ci.size()));
+  FB_TRY(dupload(m, &D.v64, A.va.data(), A.va.size()));
+  return FB_OK;
+}
+
+int upload_filter(fb_mg* m, Level& L, const std::vector<uint32_t>& f) {
+  std::vector<uint32_t> mask((L.n + 31) / 32, 0u);
+  for (uint32_t i : f) {
+    if (i >= L.n) return FB_ERR_INVALID;
+    mask[i >> 5] |= 1u << (i & 31);
+  }
+  FB_TRY(dupload(m, &L.mask, mask.data(), mask.size()));
+  FB_TRY(dupload(m, &L.filt, f.data(), f.size()));
+  L.nfilt = uint32_t(f.size());
+  return FB_OK;
+}
+
+// dense inverse of the filtered coarse matrix (Dirichlet rows/columns -> 0), Gauss-Jordan
+// with partial pivoting in FP64 on the host (setup only)
+int build_coarse_inverse(fb_mg* m, const HostCsr& A, const std::vector<uint32_t>& filt) {
+  const uint64_t n = A.rows;
+  if (n > 4096) { m->nc = 0; return FB_OK; }  // direct coarse solve limited to small coarse levels
+  std::vector<char> dir(n, 0);
+  for (auto i : filt) dir[i] = 1;
+  std::vector<double> a(n * n, 0.0), inv(n * n, 0.0);
+  for (uint64_t i = 0; i < n; ++i) {
+    inv[i * n + i] = 1.0;
+    if (dir[i]) { a[i * n + i] = 1.0; continue; }
+    for (uint64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (!dir[A.ci[k]]) a[i * n + A.ci[k]] = A.va[k];
+  }
+  for (uint64_t c = 0; c < n; ++c) {
+    uint64_t p = c;
+    for (uint64_t i = c + 1; i < n; ++i) if (std::fabs(a[i * n + c]) > std::fabs(a[p * n + c])) p = i;
+    if (a[p * n + c] == 0.0) return FB_ERR_INVALID;  // singular coarse matrix
+    if (p != c) for (uint64_t j = 0; j < n; ++j) { std::swap(a[c * n + j], a[p * n + j]); std::swap(inv[c * n + j], inv[p * n + j]); }
+    const double d = 1.0 / a[c * n + c];
+    for (uint64_t j = 0; j < n; ++j) { a[c * n + j] *= d; inv[c * n + j] *= d; }
+    for (uint64_t i = 0; i < n; ++i) {
+      if (i == c) continue;
+      const double f = a[i * n + c];
+      if (f == 0.0) continue;
+      for (uint64_t j = 0; j < n; ++j) { a[i * n + j] -= f * a[c * n + j]; inv[i * n + j] -= f * inv[c * n + j]; }
+    }
+  }
+  for (uint64_t i = 0; i < n; ++i)
+    for (uint64_t j = 0; j < n; ++j)
+      if (dir[i] || dir[j]) inv[i * n + j] = 0.0;
+  m->nc = uint32_t(n);
+  FB_TRY(dupload(m, &m->cinv64, inv.data(), inv.size()));
+  return FB_OK;
+}
+
+int common_init(fb_mg* m) {
+  FB_CUDA(cudaGetDevice(&m->device));
+  FB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  FB_TRY(dalloc(m, &m->sc, 1));
+  FB_CUDA(cudaMemset(m->sc, 0, sizeof(DevScalars)));
+  FB_TRY(dalloc(m, &m->ws, 8192));
+  FB_TRY(dalloc(m, &m->counter, 4));
+  FB_CUDA(cudaMemset(m->counter, 0, 4 * sizeof(unsigned)));
+  FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
+  FB_CUDA(cudaEventCreate(&m->ev0));
+  FB_CUDA(cudaEventCreate(&m->ev1));
+  fb_solver_cfg_default(&m->cfg);
+  return FB_OK;
+}
+
+__global__ void k_diag_sell(double* d, SellView A) {
+  const uint32_t sr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sr >= A.rows) return;
+  const uint32_t c = sr / 32, t = sr % 32;
+  const uint32_t row = A.perm ? A.perm[sr] : sr;
+  double v = 0.0;
+  const double* val = (const double*)A.val;
+  for (uint32_t j = 0; j < A.cl[c]; ++j) {
+    const uint32_t k = A.cs[c] + j * 32 + t;
+    if (A.col[k] == row && val[k] != 0.0) { v = val[k]; break; }
+  }
+  d[row] = v;
+}
+
+int finish_levels(fb_mg* m) {
+  for (auto& L : m->L) {
+    if (!L.diag) FB_TRY(dalloc(m, &L.diag, L.n));
+    k_diag_sell<<<grid_for(L.n, 256), 256, 0, m->stream>>>(L.diag, L.A.view(FB_PREC_F64));
+    FB_CHECK_LAUNCH();
+  }
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  return FB_OK;
+}
+
+// ------------------------------------------------------------------ solve
+int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info) {
+  if (!m->configured) return FB_ERR_NOT_READY;
+  FB_TRY(ensure_vectors(m, m->cfg.precision));
+  const uint32_t n = m->L[0].n;
+  cudaStream_t s = m->stream;
+  m->launches = 0;
+  FB_CUDA(cudaEventRecord(m->ev0, s));
+  FB_CUDA(cudaMemcpyAsync(m->bb, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  FB_CUDA(cudaMemcpyAsync(m->xb, sol, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  // correct(): r = filter_def(b - A x) (pcg.hpp:158-172, richardson.hpp:174-185)
+  FB_TRY(outer_defect(m));
+  if (m->cfg.outer == FB_OUTER_PCG) {
+    k_init_pcg<<<1, 1, 0, s>>>(m->sc);
+    k_fill<double><<<ew_grid(n), 256, 0, s>>>(m->p, 0.0, n);
+    m->launches += 2;
+    FB_CHECK_LAUNCH();
+  }
+  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, sizeof(double), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaStreamSynchronize(s));
+  Stop st(m->cfg.tol_rel, m->cfg.max_iter);
+  double d = std::sqrt(*m->host_rr);
+  int status = st.initial(d);
+  int it = 0;
+  if (hist) hist[0] = d;
+  while (status == 1) {
+    FB_TRY(run_body(m));
+    FB_CUDA(cudaStreamSynchronize(s));
+    ++it;
+    d = std::sqrt(*m->host_rr);
+    if (hist) hist[it] = d;
+    status = st.analyse(it, d);
+  }
+  FB_CUDA(cudaMemcpyAsync(sol, m->xb, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  FB_CUDA(cudaEventRecord(m->ev1, s));
+  FB_CUDA(cudaEventSynchronize(m->ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+  if (info) {
+    info->status = status; info->iters = it; info->def_init = st.def_init; info->def_final = d;
+    info->solve_ms = ms; info->kernel_launches = m->launches;
+  }
+  return FB_OK;
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+// ====================================================================================== C-ABI
+extern "C" {
+
+void fb_solver_cfg_default(fb_solver_cfg* c) {
+  if (!c) return;
+  c->outer = FB_OUTER_PCG;
+  c->nu = 4;
+  c->omega_jac = 0.5;
+  c->omega_rich = 1.0;
+  c->omega_outer = 1.0;
+  c->coarse = FB_COARSE_DIRECT;
+  c->tol_rel = 1e-8;
+  c->max_iter = 1000;
+  c->precision = FB_PREC_F64;
+  c->use_graphs = 1;
+}
+
+int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
+  if (!m || !c) return FB_ERR_INVALID;
+  if (c->nu < 1 || c->nu > 64 || c->max_iter < 0 || !(c->tol_rel >= 0.0) ||
+      c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3)
+    return FB_ERR_INVALID;
+  if (c->coarse == FB_COARSE_PCG) return FB_ERR_UNSUPPORTED;
+  if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;
+  FB_CUDA(cudaSetDevice(m->device));
+  const bool omega_changed = !m->configured || c->omega_jac != m->cfg.omega_jac;
+  m->cfg = *c;
+  m->configured = true;
+  if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; m->g_body_key = -1; }
+  (void)omega_changed;
+  m->prec_built = -1;
+  return ensure_vectors(m, c->precision);
+}
+
+int fb_mg_create_csr(fb_mg** out, int nl, const fb_csr_host* A, const fb_csr_host* P, const fb_csr_host* R,
+                     const uint64_t* const* filter, const uint64_t* fsize, int sigma) {
+  if (!out || nl < 1 || nl > kMaxLevels || !A || (nl > 1 && (!P || !R)) || !filter || !fsize) return FB_ERR_INVALID;
+  *out = nullptr;
+  fb_mg* m = new fb_mg();
+  int st = common_init(m);
+  if (st != FB_OK) { fb_mg_destroy(m); return st; }
+  m->L.resize(nl);
+  auto to_host = [](const fb_csr_host& c, HostCsr& h) -> bool {
+    if (!c.row_ptr || (c.nnz && (!c.col_ind || !c.val)) || c.row_ptr[c.rows] != c.nnz) return false;
+    h.rows = c.rows; h.cols = c.cols;
+    h.rp.assign(c.row_ptr, c.row_ptr + c.rows + 1);
+    h.ci.resize(c.nnz); h.va.assign(c.val, c.val + c.nnz);
+    for (uint64_t k = 0; k < c.nnz; ++k) { if (c.col_ind[k] >= c.cols) return false; h.ci[k] = uint32_t(c.col_ind[k]); }
+    return true;
+  };
+  HostCsr coarseA;
+  std::vector<uint32_t> coarseF;
+  for (int l = 0; l < nl && st == FB_OK; ++l) {
+    HostCsr h;
+    if (!to_host(A[l], h) || A[l].rows != A[l].cols || A[l].rows > 0xffffffffull) { st = FB_ERR_INVALID; break; }
+    Level& L = m->L[l];
+    L.n = uint32_t(A[l].rows);
+    std::vector<uint32_t> f(fsize[l]);
+    for (uint64_t i = 0; i < fsize[l]; ++i) f[i] = uint32_t(filter[l][i]);
+    st = upload_sell(m, L.A, h, sigma < 1 ? 1 : sigma);
+    if (st == FB_OK) st = upload_filter(m, L, f);
+    if (st == FB_OK && l + 1 < nl) {
+      HostCsr hp, hr;
+      if (!to_host(P[l], hp) || !to_host(R[l], hr) || P[l].rows != A[l].rows || P[l].cols != A[l + 1].rows ||
+          R[l].rows != A[l + 1].rows || R[l].cols != A[l].rows) { st = FB_ERR_INVALID; break; }
+      st = upload_csr(m, L.P, hp);
+      if (st == FB_OK) st = upload_csr(m, L.R, hr);
+    }
+    if (l + 1 == nl) { coarseA = std::move(h); coarseF = f; }
+  }
+  if (st == FB_OK) st = build_coarse_inverse(m, coarseA, coarseF);
+  if (st == FB_OK) st = finish_levels(m);
+  if (st != FB_OK) { fb_mg_destroy(m); return st; }
+  *out = m;
+  return FB_OK;
+}
+
+void fb_mg_destroy(fb_mg* m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->g_body) cudaGraphExecDestroy(m->g_body);
+  for (void* p : m->allocs) cudaFree(p);
+  if (m->host_rr) cudaFreeHost(m->host_rr);
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+int fb_mg_solve(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info) {
+  if (!m || !rhs || !sol) return FB_ERR_INVALID;
+  FB_CUDA(cudaSetDevice(m->device));
+  return solve_dev(m, rhs, sol, hist, info);
+}
+
+int fb_mg_solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist, fb_solve_info* info) {
+  if (!m || !rhs_h || !sol_h) return FB_ERR_INVALID;
+  if (!m->configured) return FB_ERR_NOT_READY;
+  FB_CUDA(cudaSetDevice(m->device));
+  FB_TRY(ensure_vectors(m, m->cfg.precision));
+  const uint32_t n = m->L[0].n;
+  if (!m->hb) { FB_TRY(dalloc(m, &m->hb, n)); FB_TRY(dalloc(m, &m->hx, n)); }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  FB_CUDA(cudaEventCreate(&e0));
+  FB_CUDA(cudaEventCreate(&e1));
+  FB_CUDA(cudaEventRecord(e0, m->stream));
+  FB_CUDA(cudaMemcpyAsync(m->hb, rhs_h, sizeof(double) * n, cudaMemcpyHostToDevice, m->stream));
+  FB_CUDA(cudaMemcpyAsync(m->hx, sol_h, sizeof(double) * n, cudaMemcpyHostToDevice, m->stream));
+  int st = solve_dev(m, m->hb, m->hx, hist, info);
+  if (st == FB_OK) {
+    if (cudaMemcpyAsync(sol_h, m->hx, sizeof(double) * n, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
+        cudaEventRecord(e1, m->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) st = FB_ERR_CUDA;
+  }
+  if (st == FB_OK && info) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    info->solve_ms = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st;
+}
+
+int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
+  if (!m || !def || !cor) return FB_ERR_INVALID;
+  if (!m->configured) return FB_ERR_NOT_READY;
+  FB_CUDA(cudaSetDevice(m->device));
+  FB_TRY(ensure_vectors(m, m->cfg.precision));
+  const uint32_t n = m->L[0].n;
+  cudaStream_t s = m->stream;
+  FB_CUDA(cudaMemcpyAsync(m->r, def, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, s>>>(m->r, m->r, n, m->ws, m->counter, &m->sc->rr);
+  FB_CHECK_LAUNCH();
+  const void* z = nullptr;
+  if (m->cfg.precision != FB_PREC_F64) {
+    k_cvt<float, double><<<ew_grid(n), 256, 0, s>>>(m->r32, m->r, n);
+    FB_CHECK_LAUNCH();
+  }
+  FB_TRY(precond(m, &z));
+  if (m->cfg.precision == FB_PREC_F64) FB_CUDA(cudaMemcpyAsync(cor, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  else { k_cvt<double, float><<<ew_grid(n), 256, 0, s>>>(cor, (const float*)z, n); FB_CHECK_LAUNCH(); }
+  FB_CUDA(cudaStreamSynchronize(s));
+  return FB_OK;
+}
+
+int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* ms) {
+  if (!m || !ms || level < 0 || level >= (int)m->L.size() || reps < 1 || which < 0 || which > 2 || prec < 0 || prec > 2)
+    return FB_ERR_INVALID;
+  if (!m->configured) return FB_ERR_NOT_READY;
+  FB_CUDA(cudaSetDevice(m->device));
+  Level& L = m->L[level];
+  const bool low = prec != FB_PREC_F64;
+  if ((low && !L.x32) || (!low && !L.x64) || (prec == FB_PREC_F16 && !L.A.v16) || (prec == FB_PREC_F32 && !L.A.v32))
+    return FB_ERR_NOT_READY;
+  if (which == 2 && (level != 0 || low)) return FB_ERR_INVALID;
+  const int saved = m->cfg.precision;
+  m->cfg.precision = prec;
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  auto one = [&]() -> int {
+    if (!low) {
+      double* b = level == 0 ? m->r : L.rhs64;
+      if (which == 0) { EpiJacobi<double, false> e{L.x64, b, L.invd64, L.y64, nullptr, L.mask, nullptr, m->cfg.omega_rich}; return sell_T<double>(m, L.A, L.x64, e, nullptr); }
+      if (which == 1) { EpiDefect<double, false, false> e{L.def64, b, L.mask, nullptr}; return sell_T<double>(m, L.A, L.x64, e, nullptr); }
+      EpiPcgQ<double> e{m->q, m->p, L.mask};
+      return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->p, e, &m->sc->tmp[0]);
+    }
+    float* b = level == 0 ? m->r32 : L.rhs32;
+    if (which == 0) { EpiJacobi<float, false> e{L.x32, b, L.invd32, L.y32, nullptr, L.mask, nullptr, float(m->cfg.omega_rich)}; return sell_T<float>(m, L.A, L.x32, e, nullptr); }
+    EpiDefect<float, false, false> e{L.def32, b, L.mask, nullptr};
+    return sell_T<float>(m, L.A, L.x32, e, nullptr);
+  };
+  int st = one();  // warm-up
+  if (st == FB_OK) st = cuda_status(cudaEventRecord(m->ev0, m->stream));
+  for (int i = 0; i < reps && st == FB_OK; ++i) st = one();
+  if (st == FB_OK) st = cuda_status(cudaEventRecord(m->ev1, m->stream));
+  if (st == FB_OK) st = cuda_status(cudaEventSynchronize(m->ev1));
+  m->cfg.precision = saved;
+  if (st != FB_OK) return st;
+  float t = 0.0f;
+  cudaEventElapsedTime(&t, m->ev0, m->ev1);
+  *ms = double(t) / reps;
+  return FB_OK;
+}
+
+uint64_t fb_mg_num_dofs(const fb_mg* m, int l) {
+  if (!m || l < 0 || l >= (int)m->L.size()) return 0;
+  return m->L[l].n;
+}
+int fb_mg_num_levels(const fb_mg* m) { return m ? (int)m->L.size() : 0; }
+uint64_t fb_mg_nnz(const fb_mg* m, int l) {
+  if (!m || l < 0 || l >= (int)m->L.size()) return 0;
+  return m->L[l].A.nnz;
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+// Internal types of the multigrid driver shared by fb_mg.cu and fb_assembly.cu.
+#pragma once
+#include "fb_sell.cuh"
+
+#include <vector>
+
+namespace fb {
+
+constexpr int kMaxLevels = 16;
+
+struct DevScalars {
+  double rr;            // ||r||^2 of the outer defect
+  double rz;            // latest r . z
+  double gamma;         // previous r . z (PCG)
+  double qp;            // q . p
+  double lvl[2 * kMaxLevels];  // [2l] ||rhs_l||^2, [2l+1] ||post-smoothing defect_l||^2
+  double tmp[8];
+};
+
+struct DevSell {
+  uint32_t rows = 0, cols = 0, nchunks = 0;
+  uint64_t nent = 0;      // stored entries incl. padding
+  uint64_t nnz = 0;       // true nonzeros
+  uint32_t *cs = nullptr, *cl = nullptr, *col = nullptr, *perm = nullptr;
+  uint32_t* rl = nullptr;   // row lengths (setup / export only)
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+  __half* v16 = nullptr;
+  float scale16 = 1.0f;
+  SellView view(int prec) const {
+    SellView v;
+    v.nchunks = nchunks; v.rows = rows; v.cs = cs; v.cl = cl; v.col = col; v.perm = perm;
+    v.val = prec == FB_PREC_F64 ? (const void*)v64 : (prec == FB_PREC_F32 ? (const void*)v32 : (const void*)v16);
+    v.scale = prec == FB_PREC_F16 ? scale16 : 1.0f;
+    return v;
+  }
+};
+
+struct DevCsr {
+  uint32_t rows = 0, cols = 0;
+  uint64_t nnz = 0;
+  uint32_t *rp = nullptr, *col = nullptr;
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+  CsrView view(bool f32) const {
+    CsrView v; v.rows = rows; v.rp = rp; v.col = col; v.val = f32 ? (const void*)v32 : (const void*)v64;
+    return v;
+  }
+};
+
+struct Level {
+  uint32_t n = 0;
+  DevSell A;
+  DevCsr P, R;           // P: this level <- next coarser level; R: next coarser <- this
+  double* diag = nullptr;
+  double* invd64 = nullptr;
+  float* invd32 = nullptr;
+  uint32_t* mask = nullptr;
+  uint32_t* filt = nullptr;
+  uint32_t nfilt = 0;
+  double *rhs64 = nullptr, *x64 = nullptr, *y64 = nullptr, *def64 = nullptr;
+  float *rhs32 = nullptr, *x32 = nullptr, *y32 = nullptr, *def32 = nullptr;
+  // structured info
+  int N = 0;             // cells per side
+  uint64_t ne = 0;       // elements
+  double* k = nullptr;   // per-element coefficient (device)
+};
+
+}  // namespace fb
+
+struct fb_mg {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<fb::Level> L;      // 0 = finest
+  std::vector<void*> allocs;
+  fb_solver_cfg cfg;
+  bool configured = false;
+  int prec_built = -1;           // precision whose buffers exist
+  // structured
+  bool structured = false;
+  int dim = 0, degree = 0, level = 0, level_min = 0;
+  int nloc = 0;
+  double* kref = nullptr;        // unit-coefficient element matrix on [-1,1]^d (device)
+  std::vector<double> kref_h;
+  // coarse direct solver
+  uint32_t nc = 0;
+  double* cinv64 = nullptr;
+  float* cinv32 = nullptr;
+  // outer (finest) vectors
+  double *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *xb = nullptr, *bb = nullptr;
+  float* r32 = nullptr;
+  // scalars / reduction workspace
+  fb::DevScalars* sc = nullptr;
+  double* ws = nullptr;
+  unsigned* counter = nullptr;
+  double* host_rr = nullptr;     // pinned
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // graphs
+  cudaGraphExec_t g_body = nullptr;
+  int g_body_key = -1;
+  int launches = 0;
+  int body_launches = 0;
+  double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
+  double* adj = nullptr;                 // adjoint right-hand side
+};
+
+namespace fb {
+struct HostCsr {
+  uint64_t rows = 0, cols = 0;
+  std::vector<uint64_t> rp;
+  std::vector<uint32_t> ci;
+  std::vector<double> va;
+};
+template<typename T>
+int dalloc(fb_mg* m, T** p, uint64_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc((void**)p, sizeof(T) * n) != cudaSuccess) { *p = nullptr; cudaGetLastError(); return FB_ERR_ALLOC; }
+  m->allocs.push_back(*p);
+  return FB_OK;
+}
+template<typename T>
+int dupload(fb_mg* m, T** p, const T* h, uint64_t n) {
+  int st = dalloc(m, p, n);
+  if (st != FB_OK) return st;
+  if (n && cudaMemcpy(*p, h, sizeof(T) * n, cudaMemcpyHostToDevice) != cudaSuccess) return FB_ERR_CUDA;
+  return FB_OK;
+}
+int common_init(fb_mg* m);
+int finish_levels(fb_mg* m);
+int build_coarse_inverse(fb_mg* m, const HostCsr& A, const std::vector<uint32_t>& filt);
+int upload_sell(fb_mg* m, DevSell& S, const HostCsr& A, int sigma);
+int upload_csr(fb_mg* m, DevCsr& D, const HostCsr& A);
+int upload_filter(fb_mg* m, Level& L, const std::vector<uint32_t>& f);
+int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info);
+unsigned ew_grid(uint64_t n);
+}  // namespace fb

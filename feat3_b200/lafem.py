@@ -1,0 +1,231 @@
+"""Device containers mirroring FEAT3's LAFEM interface for the multigrid path.
+
+``SparseMatrixCSR.apply``, ``SparseMatrixELL.apply``, ``DenseVector.axpy/dot/norm2/...``,
+``UnitFilter.filter_*`` and ``Transfer.prol/rest`` keep the reference's names and argument
+meaning (kernel/lafem/sparse_matrix_csr.hpp:1899-2010, sparse_matrix_ell.hpp:1983-2014,
+dense_vector.hpp:883-1031, unit_filter.hpp:399-437, transfer.hpp:249-285) and run on the
+sm_100a kernels of ``libfeat3_b200.so``. Device memory comes from torch (plumbing only);
+every computation is a C-ABI call.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_EPS = {torch.float64: np.finfo(np.float64).eps, torch.float32: np.finfo(np.float32).eps}
+
+
+def _sfx(dtype):
+    if dtype == torch.float64:
+        return "f64"
+    if dtype == torch.float32:
+        return "f32"
+    raise TypeError(f"unsupported dtype {dtype}")
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+def _dev(x, dtype):
+    return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).cuda()
+
+
+class DenseVector:
+    """DenseVector<Mem::CUDA, DT> (kernel/lafem/dense_vector.hpp)."""
+
+    def __init__(self, data):
+        if isinstance(data, torch.Tensor):
+            self.t = data
+        else:
+            self.t = torch.as_tensor(np.ascontiguousarray(data)).cuda()
+        if not self.t.is_cuda or not self.t.is_contiguous():
+            raise ValueError("DenseVector needs a contiguous CUDA tensor")
+
+    @classmethod
+    def zeros(cls, n, dtype=torch.float64):
+        return cls(torch.zeros(n, dtype=dtype, device="cuda"))
+
+    @property
+    def dtype(self):
+        return self.t.dtype
+
+    def size(self):
+        return self.t.numel()
+
+    def numpy(self):
+        return self.t.detach().cpu().numpy()
+
+    def _f(self, name):
+        return f"fb_{name}_{_sfx(self.dtype)}"
+
+    # this = alpha*x + y  (dense_vector.hpp:883-905)
+    def axpy(self, x, y, alpha=1.0):
+        _lib.call(self._f("axpy"), _p(self.t), alpha, _p(x.t), _p(y.t), self.size(), _stream())
+        return self
+
+    def dot(self, x):
+        out = _lib.C.c_double(0.0)
+        _lib.call(self._f("dot") + "_sync", _p(self.t), _p(x.t), self.size(), _lib.C.byref(out), _stream())
+        return out.value
+
+    def norm2(self):
+        out = _lib.C.c_double(0.0)
+        _lib.call(self._f("norm2") + "_sync", _p(self.t), self.size(), _lib.C.byref(out), _stream())
+        return out.value
+
+    def component_product(self, x, y):
+        _lib.call(self._f("component_product"), _p(self.t), _p(x.t), _p(y.t), self.size(), _stream())
+        return self
+
+    def component_invert(self, x, alpha=1.0):
+        _lib.call(self._f("component_invert"), _p(self.t), _p(x.t), alpha, self.size(), _stream())
+        return self
+
+    def scale(self, x, s):
+        _lib.call(self._f("scale"), _p(self.t), _p(x.t), s, self.size(), _stream())
+        return self
+
+    def format(self, value=0.0):
+        _lib.call(f"fb_set_{_sfx(self.dtype)}", _p(self.t), value, self.size(), _stream())
+        return self
+
+    def copy(self, x):
+        self.t.copy_(x.t)
+        return self
+
+    def convert(self, x):
+        """precision conversion (MemoryPool<Mem::CUDA>::convert)"""
+        if self.dtype == x.dtype:
+            return self.copy(x)
+        fn = "fb_convert_f64_to_f32" if self.dtype == torch.float32 else "fb_convert_f32_to_f64"
+        _lib.call(fn, _p(self.t), _p(x.t), self.size(), _stream())
+        return self
+
+
+class SparseMatrixCSR:
+    """SparseMatrixCSR<Mem::CUDA, DT, u32> with the reference's apply semantics."""
+
+    def __init__(self, row_ptr, col_ind, val, columns=None, dtype=torch.float64):
+        rp = np.asarray(row_ptr)
+        self.rows = rp.size - 1
+        self.columns = int(columns if columns is not None else self.rows)
+        self.nnz = int(rp[-1])
+        if self.nnz >= 2 ** 32 or self.rows >= 2 ** 32:
+            raise ValueError("32-bit index range exceeded")
+        self.row_ptr = _dev(rp.astype(np.uint32).view(np.int32), torch.int32)
+        self.col_ind = _dev(np.asarray(col_ind).astype(np.uint32).view(np.int32), torch.int32)
+        self.val = _dev(np.asarray(val, dtype=np.float64), dtype)
+
+    @property
+    def dtype(self):
+        return self.val.dtype
+
+    # r = y + alpha*A*x  (sparse_matrix_csr.hpp:1973-2010);  r = A*x when y is None (:1899-1928)
+    def apply(self, r, x, y=None, alpha=1.0, transposed=False):
+        b = 0.0 if y is None else 1.0
+        _lib.call(f"fb_csr_apply_{_sfx(self.dtype)}", _p(r.t), alpha, _p(x.t), b, _p(y.t if y is not None else None),
+                  _p(self.val), _p(self.col_ind), _p(self.row_ptr), self.rows, self.columns, self.nnz,
+                  1 if transposed else 0, _stream())
+        return r
+
+    def apply_raw(self, r, a, x, b, y, transposed=False):
+        """Arch::Apply::csr signature: r = b*y + a*A*x"""
+        _lib.call(f"fb_csr_apply_{_sfx(self.dtype)}", _p(r.t), a, _p(x.t), b, _p(y.t if y is not None else None),
+                  _p(self.val), _p(self.col_ind), _p(self.row_ptr), self.rows, self.columns, self.nnz,
+                  1 if transposed else 0, _stream())
+        return r
+
+    def extract_diag(self, d):
+        _lib.call(f"fb_diagonal_csr_{_sfx(self.dtype)}", _p(d.t), _p(self.val), _p(self.col_ind), _p(self.row_ptr),
+                  self.rows, _stream())
+        return d
+
+
+class SparseMatrixELL:
+    """SparseMatrixELL<Mem::CUDA, DT, u32>: FEAT's SELL-C layout (sparse_matrix_ell.hpp:38-63, 865-960)."""
+
+    def __init__(self, row_ptr, col_ind, val, columns=None, C=32, dtype=torch.float64):
+        rp = np.asarray(row_ptr, dtype=np.int64)
+        ci = np.asarray(col_ind, dtype=np.int64)
+        va = np.asarray(val, dtype=np.float64)
+        self.rows = rp.size - 1
+        self.columns = int(columns if columns is not None else self.rows)
+        self.C = C
+        nchunks = (self.rows + C - 1) // C
+        rl = np.diff(rp)
+        cl = np.zeros(nchunks, np.int64)
+        for c in range(nchunks):
+            cl[c] = rl[c * C:(c + 1) * C].max(initial=0)
+        cs = np.zeros(nchunks + 1, np.int64)
+        cs[1:] = np.cumsum(cl * C)
+        vs = int(cs[-1])
+        cval = np.zeros(vs)
+        ccol = np.zeros(vs, np.int64)
+        for i in range(self.rows):
+            c, t = divmod(i, C)
+            k = np.arange(rl[i])
+            ccol[cs[c] + t + k * C] = ci[rp[i]:rp[i + 1]]
+            cval[cs[c] + t + k * C] = va[rp[i]:rp[i + 1]]
+        self.val = _dev(cval, dtype)
+        self.col_ind = _dev(ccol.astype(np.uint32).view(np.int32), torch.int32)
+        self.cs = _dev(cs.astype(np.uint32).view(np.int32), torch.int32)
+        self.cl = _dev(cl.astype(np.uint32).view(np.int32), torch.int32)
+
+    @property
+    def dtype(self):
+        return self.val.dtype
+
+    def apply(self, r, x, y=None, alpha=1.0):
+        b = 0.0 if y is None else 1.0
+        _lib.call(f"fb_ell_apply_{_sfx(self.dtype)}", _p(r.t), alpha, _p(x.t), b, _p(y.t if y is not None else None),
+                  _p(self.val), _p(self.col_ind), _p(self.cs), _p(self.cl), self.C, self.rows, _stream())
+        return r
+
+    def extract_diag(self, d):
+        if self.dtype != torch.float64:
+            raise TypeError("extract_diag is provided for FP64 ELL matrices")
+        _lib.call("fb_diagonal_ell_f64", _p(d.t), _p(self.val), _p(self.col_ind), _p(self.cs), _p(self.cl),
+                  self.C, self.rows, _stream())
+        return d
+
+
+class UnitFilter:
+    """UnitFilter<Mem::CUDA, DT, u32> (kernel/lafem/unit_filter.hpp)."""
+
+    def __init__(self, indices, values=None, dtype=torch.float64):
+        idx = np.asarray(indices, dtype=np.int64)
+        self.ue = idx.size
+        self.idx = _dev(idx.astype(np.uint32).view(np.int32), torch.int32)
+        self.sv = _dev(np.zeros(self.ue) if values is None else np.asarray(values, np.float64), dtype)
+
+    def filter_rhs(self, v):
+        _lib.call(f"fb_unit_filter_rhs_{_sfx(v.dtype)}", _p(v.t), _p(self.sv), _p(self.idx), self.ue, _stream())
+        return v
+
+    filter_sol = filter_rhs
+
+    def filter_def(self, v):
+        _lib.call(f"fb_unit_filter_def_{_sfx(v.dtype)}", _p(v.t), _p(self.idx), self.ue, _stream())
+        return v
+
+    filter_cor = filter_def
+
+
+class Transfer:
+    """LAFEM::Transfer (kernel/lafem/transfer.hpp:28-313): explicit P and R = P^T."""
+
+    def __init__(self, prol: SparseMatrixCSR, rest: SparseMatrixCSR):
+        self.prol_mat, self.rest_mat = prol, rest
+
+    def prol(self, v_fine, v_coarse):
+        return self.prol_mat.apply(v_fine, v_coarse)
+
+    def rest(self, v_fine, v_coarse):
+        return self.rest_mat.apply(v_coarse, v_fine)

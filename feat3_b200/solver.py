@@ -1,0 +1,187 @@
+"""Python face of the native multigrid driver (solver layer of the C-ABI).
+
+The composition mirrors the reference's solver trees: ``PCG(MultiGrid(V; Richardson(Jacobi)
+smoothers; coarse solver))`` of applications/poisson_dirichlet.cpp:152-190 and
+``Richardson(MultiGrid)`` of tutorials/tutorial_05_multigrid.cpp:373-449, with the mixed
+form ``Richardson/PCG(ConvertPrecond(MultiGrid<float>))`` of
+kernel/solver/convert_precond.hpp:41-120. The status codes are the reference's
+``Solver::Status`` (kernel/solver/base.hpp:48-64).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+
+STATUS = {0: "undefined", 1: "progress", 2: "success", 3: "aborted", 4: "diverged", 5: "max_iter", 6: "stagnated"}
+OUTER = {"pcg": 0, "richardson": 1}
+COARSE = {"direct": 0, "pcg": 1, "smoother": 2, "none": 3}
+PRECISION = {"f64": 0, "f32": 1, "f16": 2}
+RHS = {"sine": 0, "one": 1, "expbubble": 2}
+
+
+def _stream_sync():
+    torch.cuda.synchronize()
+
+
+class MultiGrid:
+    """A device multigrid hierarchy plus its outer solver."""
+
+    def __init__(self, handle, structured):
+        self.h = handle
+        self.structured = structured
+        self.cfg = None
+
+    # ---------------------------------------------------------------- construction
+    @classmethod
+    def structured(cls, dim, degree, level, level_min=1, k=None, sell_sigma=1):
+        lib = _lib.load()
+        karr = None
+        desc = _lib.StructuredDesc(dim, degree, level, level_min, None, 0, sell_sigma)
+        if k is not None:
+            if isinstance(k, torch.Tensor) and k.is_cuda:
+                karr = k.contiguous().to(torch.float64)
+                desc.k, desc.k_on_device = karr.data_ptr(), 1
+            else:
+                karr = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
+                desc.k = karr.ctypes.data
+        h = C.c_void_p()
+        _lib.check("fb_mg_create_structured", lib.fb_mg_create_structured(C.byref(h), C.byref(desc)))
+        mg = cls(h, True)
+        mg.dim, mg.degree, mg.level, mg.level_min = dim, degree, level, level_min
+        return mg
+
+    @classmethod
+    def from_csr(cls, levels, sell_sigma=1):
+        """levels: finest first; each a dict with A=(row_ptr, col_ind, val), filter=indices and,
+        except on the coarsest level, P=(...) mapping the next level onto this one and R=(...)."""
+        lib = _lib.load()
+        nl = len(levels)
+        keep = []
+
+        def csr(t, rows, cols):
+            rp = np.ascontiguousarray(np.asarray(t[0], dtype=np.uint64))
+            ci = np.ascontiguousarray(np.asarray(t[1], dtype=np.uint64))
+            va = np.ascontiguousarray(np.asarray(t[2], dtype=np.float64))
+            keep.extend([rp, ci, va])
+            return _lib.CsrHost(rows, cols, int(rp[-1]), rp.ctypes.data, ci.ctypes.data, va.ctypes.data)
+
+        n = [len(l["A"][0]) - 1 for l in levels]
+        A = (_lib.CsrHost * nl)(*[csr(l["A"], n[i], n[i]) for i, l in enumerate(levels)])
+        P = (_lib.CsrHost * max(nl - 1, 1))()
+        R = (_lib.CsrHost * max(nl - 1, 1))()
+        for i in range(nl - 1):
+            P[i] = csr(levels[i]["P"], n[i], n[i + 1])
+            R[i] = csr(levels[i]["R"], n[i + 1], n[i])
+        filt = [np.ascontiguousarray(np.asarray(l["filter"], dtype=np.uint64)) for l in levels]
+        fptr = (C.c_void_p * nl)(*[f.ctypes.data if f.size else None for f in filt])
+        fsz = (C.c_uint64 * nl)(*[f.size for f in filt])
+        h = C.c_void_p()
+        rc = lib.fb_mg_create_csr(C.byref(h), nl, C.cast(A, C.c_void_p), C.cast(P, C.c_void_p),
+                                  C.cast(R, C.c_void_p), C.cast(fptr, C.c_void_p), C.cast(fsz, C.c_void_p),
+                                  sell_sigma)
+        _lib.check("fb_mg_create_csr", rc)
+        return cls(h, False)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().fb_mg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- configuration
+    def configure(self, outer="pcg", nu=4, omega_jac=0.5, omega_rich=1.0, omega_outer=1.0, coarse="direct",
+                  tol=1e-8, max_iter=1000, precision="f64", graphs=True):
+        cfg = _lib.SolverCfg(OUTER[outer], nu, omega_jac, omega_rich, omega_outer, COARSE[coarse], tol, max_iter,
+                             PRECISION[precision], 1 if graphs else 0)
+        _lib.check("fb_mg_configure", _lib.load().fb_mg_configure(self.h, C.byref(cfg)))
+        self.cfg = cfg
+        return self
+
+    # ---------------------------------------------------------------- queries
+    def num_levels(self):
+        return _lib.load().fb_mg_num_levels(self.h)
+
+    def ndofs(self, level=0):
+        return int(_lib.load().fb_mg_num_dofs(self.h, level))
+
+    def nnz(self, level=0):
+        return int(_lib.load().fb_mg_nnz(self.h, level))
+
+    def export_csr(self, level=0):
+        n, nnz = self.ndofs(level), self.nnz(level)
+        rp = np.zeros(n + 1, np.uint64)
+        ci = np.zeros(nnz, np.uint32)
+        va = np.zeros(nnz)
+        _lib.call("fb_mg_export_csr", self.h, level, rp.ctypes.data, ci.ctypes.data, va.ctypes.data)
+        return rp.astype(np.int64), ci.astype(np.int64), va
+
+    # ---------------------------------------------------------------- work
+    def assemble_rhs(self, kind="sine"):
+        b = torch.zeros(self.ndofs(), dtype=torch.float64, device="cuda")
+        _lib.call("fb_mg_assemble_rhs", self.h, RHS[kind], b.data_ptr())
+        return b
+
+    def _info(self, info, hist):
+        it = info.iters
+        return {"status": STATUS.get(info.status, info.status), "iters": it, "def_init": info.def_init,
+                "def_final": info.def_final, "solve_ms": info.solve_ms, "kernel_launches": info.kernel_launches,
+                "hist": None if hist is None else hist[: it + 1].copy()}
+
+    def solve(self, rhs, sol=None, record=True):
+        """Solver::solve(solver, sol, rhs) on device tensors; sol is updated in place."""
+        if self.cfg is None:
+            self.configure()
+        if sol is None:
+            sol = torch.zeros_like(rhs)
+        hist = np.zeros(self.cfg.max_iter + 1) if record else None
+        info = _lib.SolveInfo()
+        torch.cuda.current_stream().synchronize()
+        _lib.call("fb_mg_solve", self.h, rhs.data_ptr(), sol.data_ptr(),
+                  None if hist is None else hist.ctypes.data, C.byref(info))
+        out = self._info(info, hist)
+        out["u"] = sol
+        return out
+
+    def solve_host(self, rhs, sol=None, record=True):
+        """End-to-end: host buffers in, host solution out (copies inside the timed region)."""
+        if self.cfg is None:
+            self.configure()
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        sol = np.zeros_like(rhs) if sol is None else np.ascontiguousarray(sol, dtype=np.float64)
+        hist = np.zeros(self.cfg.max_iter + 1) if record else None
+        info = _lib.SolveInfo()
+        _lib.call("fb_mg_solve_host", self.h, rhs.ctypes.data, sol.ctypes.data,
+                  None if hist is None else hist.ctypes.data, C.byref(info))
+        out = self._info(info, hist)
+        out["u"] = sol
+        return out
+
+    def vcycle(self, d):
+        cor = torch.empty_like(d)
+        _lib.call("fb_mg_vcycle", self.h, d.data_ptr(), cor.data_ptr())
+        return cor
+
+    def element_grad(self, u, lam):
+        ne = (1 << self.level) ** self.dim
+        g = torch.empty(ne, dtype=torch.float64, device="cuda")
+        _lib.call("fb_mg_element_grad", self.h, u.data_ptr(), lam.data_ptr(), g.data_ptr())
+        return g
+
+    def adjoint_grad(self, u, u_target):
+        """lambda = (A^T)^-1 filter(u - u_target) by the configured MG solver; dJ/dk per element."""
+        ne = (1 << self.level) ** self.dim
+        lam = torch.empty_like(u)
+        g = torch.empty(ne, dtype=torch.float64, device="cuda")
+        info = _lib.SolveInfo()
+        _lib.call("fb_mg_adjoint_grad", self.h, u.data_ptr(), u_target.data_ptr(), lam.data_ptr(), g.data_ptr(),
+                  C.byref(info))
+        return lam, g, self._info(info, None)

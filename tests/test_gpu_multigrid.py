@@ -1,0 +1,175 @@
+"""Solver-layer parity on the GPU against the oracle restatement (itself pinned to the
+reference's own solver by tests/test_oracle_golden.py): identical iteration counts and the
+solution within 1e-10 relative for the FP64 drop-in; error <= 1e-8 against the FP64 oracle
+for the mixed forms."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+TOL_U = 1e-10
+
+
+def relerr(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
+
+
+def lognormal_k(dim, level, sigma=1.0, seed=0):
+    n = (1 << level) ** dim
+    return np.exp(sigma * np.random.default_rng(seed).standard_normal(n))
+
+
+CASES = [
+    # dim, degree, level, level_min, rhs, k-sigma, nu, omega_jac, coarse
+    (2, 1, 7, 1, "sine", None, 4, 0.5, "direct"),        # C1
+    (3, 1, 4, 1, "sine", None, 2, 0.5, "direct"),        # C2 shape, smaller
+    (2, 2, 5, 1, "one", 1.0, 2, 0.5, "direct"),          # C3 shape, smaller
+    (2, 1, 6, 1, "one", 0.5, 2, 0.5, "direct"),          # C4 shape, smaller
+    (3, 1, 4, 1, "one", 1.0, 2, 0.5, "direct"),          # C5 shape, smaller
+    (3, 2, 3, 1, "one", 1.0, 2, 0.5, "direct"),          # 3D Q2
+    (2, 1, 5, 0, "expbubble", None, 4, 0.7, "smoother"),  # poisson_dirichlet composition
+    (2, 1, 6, 2, "sine", None, 1, 0.5, "none"),          # nu = 1 paths, identity coarse solver
+    (2, 1, 6, 2, "sine", None, 3, 0.5, "smoother"),      # odd nu, smoother coarse solver
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"d{c[0]}q{c[1]}L{c[2]}-{c[4]}-k{c[5]}-nu{c[6]}-{c[8]}" for c in CASES])
+@pytest.mark.parametrize("graphs", [True, False])
+def test_structured_pcg_matches_oracle(case, graphs):
+    from feat3_b200.solver import MultiGrid
+    dim, deg, lvl, lmin, rhs, ks, nu, wj, coarse = case
+    k = None if ks is None else lognormal_k(dim, lvl, ks, seed=lvl)
+    H = po.Hierarchy(dim, deg, lvl, lmin, k)
+    b = H.rhs(rhs)
+    ref = H.solve(b, nu=nu, omega_jac=wj, coarse=coarse)
+    mg = MultiGrid.structured(dim, deg, lvl, lmin, k)
+    mg.configure(nu=nu, omega_jac=wj, coarse=coarse, graphs=graphs)
+    bg = mg.assemble_rhs(rhs)
+    np.testing.assert_allclose(bg.cpu().numpy(), b, rtol=1e-12, atol=1e-15 * np.abs(b).max())
+    res = mg.solve(torch.tensor(b).cuda())
+    assert res["status"] == ref["status"] == "success"
+    assert res["iters"] == ref["iters"]
+    np.testing.assert_allclose(res["hist"], ref["hist"], rtol=1e-6)
+    assert relerr(res["u"].cpu().numpy(), ref["u"]) <= TOL_U
+
+
+@pytest.mark.parametrize("dim,deg,lvl", [(2, 1, 5), (2, 2, 4), (3, 1, 3), (3, 2, 2)])
+def test_structured_assembly_bitwise(dim, deg, lvl):
+    """device assembly reproduces the cell-wise scatter assembly entry for entry"""
+    from feat3_b200.solver import MultiGrid
+    k = lognormal_k(dim, lvl, 1.0, seed=7)
+    H = po.Hierarchy(dim, deg, lvl, 1, k)
+    mg = MultiGrid.structured(dim, deg, lvl, 1, k)
+    for l in range(mg.num_levels()):
+        rp, ci, va = mg.export_csr(l)
+        orp, oci, ova = H.csr(lvl - l)
+        np.testing.assert_array_equal(rp, orp)
+        np.testing.assert_array_equal(ci, oci)
+        np.testing.assert_array_equal(va, ova)
+
+
+@pytest.mark.parametrize("sigma", [1, 256])
+def test_csr_hierarchy_dropin(sigma):
+    """a hierarchy handed over as CSR matrices (push_level semantics), SELL-C-sigma inside"""
+    from feat3_b200.solver import MultiGrid
+    k = lognormal_k(2, 6, 1.0, seed=3)
+    H = po.Hierarchy(2, 2, 6, 2, k)
+    levels = []
+    for l in range(6, 1, -1):
+        d = {"A": H.csr(l), "filter": H.filter(l)}
+        if l > 2:
+            d["P"], d["R"] = H.prol(l), H.rest(l)
+        levels.append(d)
+    b = H.rhs("one")
+    ref = H.solve(b, nu=2)
+    mg = MultiGrid.from_csr(levels, sell_sigma=sigma)
+    mg.configure(nu=2)
+    res = mg.solve(torch.tensor(b).cuda())
+    assert res["iters"] == ref["iters"]
+    assert relerr(res["u"].cpu().numpy(), ref["u"]) <= TOL_U
+
+
+@pytest.mark.parametrize("outer", ["richardson", "pcg"])
+def test_richardson_outer(outer):
+    from feat3_b200.solver import MultiGrid
+    H = po.Hierarchy(2, 1, 7, 1)
+    b = H.rhs("sine")
+    kw = dict(nu=4, omega_jac=1.0, omega_rich=0.8, coarse="direct")
+    ref = H.solve(b, solver=outer, **kw)
+    mg = MultiGrid.structured(2, 1, 7, 1)
+    mg.configure(outer=outer, **kw)
+    res = mg.solve(torch.tensor(b).cuda())
+    assert res["iters"] == ref["iters"]
+    assert relerr(res["u"].cpu().numpy(), ref["u"]) <= TOL_U
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16"])
+@pytest.mark.parametrize("outer", ["richardson", "pcg"])
+def test_mixed_precision_error(prec, outer):
+    from feat3_b200.solver import MultiGrid
+    k = lognormal_k(3, 5, 1.0, seed=5)
+    H = po.Hierarchy(3, 1, 5, 1, k)
+    b = H.rhs("one")
+    ref = H.solve(b, nu=2, tol=1e-12)
+    mg = MultiGrid.structured(3, 1, 5, 1, k)
+    mg.configure(nu=2, precision=prec, outer=outer)
+    res = mg.solve(torch.tensor(b).cuda())
+    assert res["status"] == "success"
+    assert res["hist"][-1] <= 1e-8 * res["hist"][0]
+    assert relerr(res["u"].cpu().numpy(), ref["u"]) <= 1e-8
+
+
+def test_host_buffer_solve_matches_device_solve():
+    from feat3_b200.solver import MultiGrid
+    mg = MultiGrid.structured(2, 1, 6, 1).configure(nu=2)
+    b = mg.assemble_rhs("sine")
+    r1 = mg.solve(b)
+    r2 = mg.solve_host(b.cpu().numpy())
+    assert r1["iters"] == r2["iters"]
+    np.testing.assert_array_equal(r1["u"].cpu().numpy(), r2["u"])
+
+
+def test_zero_rhs_and_nan_status():
+    """initial defect <= eps^2 -> success at once; a NaN defect -> aborted (iterative.hpp:744-766)"""
+    from feat3_b200.solver import MultiGrid
+    mg = MultiGrid.structured(2, 1, 5, 1).configure(nu=2)
+    z = torch.zeros(mg.ndofs(), dtype=torch.float64, device="cuda")
+    r = mg.solve(z)
+    assert r["status"] == "success" and r["iters"] == 0
+    b = mg.assemble_rhs("sine")
+    b[100] = float("nan")
+    r = mg.solve(b)
+    assert r["status"] == "aborted"
+
+
+def test_vcycle_matches_oracle():
+    from feat3_b200.solver import MultiGrid
+    H = po.Hierarchy(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11))
+    d = H.rhs("one")
+    ref = H.vcycle(d, nu=2)
+    mg = MultiGrid.structured(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11)).configure(nu=2)
+    cor = mg.vcycle(torch.tensor(d).cuda()).cpu().numpy()
+    assert relerr(cor, ref) <= 1e-13
+
+
+def test_adjoint_gradient_matches_oracle():
+    from feat3_b200.solver import MultiGrid
+    lvl = 6
+    k = lognormal_k(2, lvl, 0.5, seed=21)
+    H = po.Hierarchy(2, 1, lvl, 1, k)
+    b = H.rhs("one")
+    u = H.solve(b, nu=2, tol=1e-14)["u"]
+    ut = H.solve(b * 0 + H.rhs("one"), nu=2, tol=1e-14)["u"] * 0.9
+    g = u - ut
+    g[H.filter()] = 0.0
+    lam = H.solve(g, nu=2, tol=1e-14)["u"]
+    gref = H.element_grad(u, lam)
+    mg = MultiGrid.structured(2, 1, lvl, 1, k).configure(nu=2, tol=1e-14)
+    ud = mg.solve(torch.tensor(b).cuda())["u"]
+    lam_d, gd, info = mg.adjoint_grad(ud, torch.tensor(ut).cuda())
+    assert info["status"] == "success"
+    assert relerr(lam_d.cpu().numpy(), lam) <= 1e-10
+    assert relerr(gd.cpu().numpy(), gref) <= 1e-10
