@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--cpu-level", type=int, default=6, help="size of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default=None,
+                    help="profiling aid, e.g. f16, f64-sell, f16-stencil: run just this form's timed solves")
     return ap.parse_args()
 
 
@@ -184,8 +186,8 @@ def native_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def run_form(prec, steps, warmup, host=False):
-        mg.configure(precision=prec, **common)
+    def run_form(prec, steps, warmup, host=False, fmt="stencil"):
+        mg.configure(precision=prec, format=fmt, **common)
         hb = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
         hx = torch.zeros(n, dtype=torch.float64).pin_memory().numpy()
         hb[:] = rhs.cpu().numpy()
@@ -208,33 +210,41 @@ def native_arm(args):
         wall = time.time() - t_wall
         return res, times, launches, iters, wall
 
-    # --- FP64 drop-in form
-    r64, t64, l64, it64, _ = run_form("f64", args.steps, args.warmup)
+    if args.only:
+        prec, _, fmt = args.only.partition("-")
+        r, t, l, it, _ = run_form(prec, args.steps, args.warmup, fmt=fmt or "stencil")
+        if rank == 0:
+            print(json.dumps({"form": args.only, "time_s": float(np.median(t)), "iters": it[-1], "launches": l,
+                              "dofs": n, "level": level}))
+        mg.close()
+        return 0
+    # --- FP64 forms: the drop-in (SELL-C-sigma, CSR transfers) and the same on the stencil storage
+    r64, t64, l64, it64, _ = run_form("f64", args.steps, args.warmup, fmt="sell")
     u64 = r64["u"].clone()
+    r64s, t64s, _, it64s, _ = run_form("f64", args.steps, args.warmup, fmt="stencil")
     # --- mixed form (headline)
     clk = ClockSampler(local)
     clk.start()
-    rmx, tmx, lmx, itmx, wall = run_form("f16", args.steps, args.warmup)
+    rmx, tmx, lmx, itmx, wall = run_form("f16", args.steps, args.warmup, fmt="stencil")
     clocks = clk.stop()
     umx = rmx["u"]
     err = float(torch.linalg.norm(umx - u64) / torch.linalg.norm(u64))
     # --- end to end through the host-buffer entry point
-    re2e, te2e, _, _, _ = run_form("f16", max(2, args.steps // 2), 1, host=True)
+    re2e, te2e, _, _, _ = run_form("f16", max(2, args.steps // 2), 1, host=True, fmt="stencil")
 
-    # --- roofline of the dominant kernel (finest-level FP16 fused defect+Jacobi SpMV)
+    # --- roofline of the finest-level SpMV kernels (CUDA events on the solver stream)
     nnz = mg.nnz(0)
     rf = {}
-    for name, prec, which, sv, sx in (("sell_jacobi_f16", 2, 0, 2, 4), ("sell_jacobi_f64", 0, 0, 8, 8),
-                                      ("sell_pcgq_f64", 0, 2, 8, 8)):
-        mg.configure(precision="f64" if prec == 0 else "f16", **common)
+    for name, prec, fmt, which, sv, si, sx in (
+            ("stencil_jacobi_f16", "f16", "stencil", 0, 2, 0, 4), ("stencil_jacobi_f64", "f64", "stencil", 0, 8, 0, 8),
+            ("stencil_pcgq_f64", "f64", "stencil", 2, 8, 0, 8), ("sell_jacobi_f64", "f64", "sell", 0, 8, 4, 8),
+            ("sell_pcgq_f64", "f64", "sell", 2, 8, 4, 8), ("sell_jacobi_f16", "f16", "sell", 0, 2, 4, 4)):
+        mg.configure(precision=prec, format=fmt, **common)
         ms = C.c_double(0.0)
-        _lib.call("fb_mg_time_spmv", mg.h, 0, which, prec, 20, C.byref(ms))
-        # algorithmic bytes: nnz*(s_v + 4) + x once + per-row vector streams
-        if which == 0:
-            vec = n * (sx + sx + sx + sx)  # x (own row read), rhs, invd, out
-        else:
-            vec = n * (sx + sx)            # p, q
-        alg = nnz * (sv + 4) + n * sx + vec + n / 8
+        _lib.call("fb_mg_time_spmv", mg.h, 0, which, {"f64": 0, "f32": 1, "f16": 2}[prec], 20, C.byref(ms))
+        # algorithmic bytes: nnz*(value + index) + x once + the row streams of the epilogue + mask
+        vec = n * sx * (3 if which == 0 else 2)  # Jacobi: rhs, invd, out; PCG q: p (own row), q
+        alg = nnz * (sv + si) + n * sx + vec + n / 8
         rf[name] = {"ms": ms.value, "bytes": alg, "GBps": alg / (ms.value * 1e-3) / 1e9}
     peaks = {}
     try:
@@ -243,10 +253,11 @@ def native_arm(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    dom = rf["sell_jacobi_f16"]
+    dom = rf["stencil_jacobi_f16"]
 
     t_mixed = max_over_ranks(float(np.median(tmx)))
     t_fp64 = max_over_ranks(float(np.median(t64)))
+    t_fp64s = max_over_ranks(float(np.median(t64s)))
     t_e2e = max_over_ranks(float(np.median(te2e)))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -263,14 +274,19 @@ def native_arm(args):
             "mixed": {"time_s": t_mixed, "iters": itmx[-1], "err_vs_fp64": err,
                       "dof_it_per_s": n * itmx[-1] / t_mixed, "final_rel_residual": rmx["hist"][-1] / rmx["hist"][0]},
             "fp64": {"time_s": t_fp64, "iters": it64[-1], "dof_it_per_s": n * it64[-1] / t_fp64,
-                     "final_rel_residual": r64["hist"][-1] / r64["hist"][0]},
+                     "final_rel_residual": r64["hist"][-1] / r64["hist"][0],
+                     "storage": "SELL-C-sigma (C=32, 32-bit column indices) + CSR transfers (drop-in form)"},
+            "fp64_stencil": {"time_s": t_fp64s, "iters": it64s[-1], "dof_it_per_s": n * it64s[-1] / t_fp64s,
+                             "storage": "SELL-32 with implicit stencil columns + matrix-free Q1 transfers"},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+            "speedup_mixed_vs_fp64_same_storage": t_fp64s / t_mixed,
             "roofline": {"bound": "hbm", "achieved": dom["GBps"], "peak": peak, "unit": "GB/s",
-                         "frac": dom["GBps"] / peak, "traffic": None, "kernel": "k_sell<__half,float,float,EpiJacobi> finest level",
+                         "frac": dom["GBps"] / peak, "traffic": None, "kernel": "k_stencil<__half,float,float,EpiJacobi,27> finest level (FP16 values, implicit columns)",
                          "kernels": rf, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650"},
             "cpu_baseline": cpu,
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
-            "gpu_launches": lmx // max(1, args.steps),
+            "gpu_launches": lmx,
+            "gpu_launches_per_step": lmx // max(1, args.steps),
             "clocks": clocks, "setup_s": setup_s,
             "wall_s_mixed_steps": wall,
         }

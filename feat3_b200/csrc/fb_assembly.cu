@@ -24,6 +24,14 @@
 #include <cstring>
 #include <vector>
 
+#undef FB_CHECK_LAUNCH
+#define FB_CHECK_LAUNCH()                                                              \
+  do {                                                                                 \
+    cudaError_t _e = cudaGetLastError();                                               \
+    if (_e == cudaSuccess && fb::debug_enabled()) _e = fb::debug_sync(m->stream, __FILE__, __LINE__); \
+    if (_e != cudaSuccess) return FB_ERR_CUDA;                                         \
+  } while (0)
+
 namespace fb {
 
 struct Geom {
@@ -109,7 +117,12 @@ __host__ __device__ inline void row_entries(uint64_t row, const Geom& g, const d
               if (!inside) continue;
               const uint64_t eidx = uint64_t(e3[0]) + uint64_t(g.N) * (uint64_t(e3[1]) + uint64_t(g.N) * e3[2]);
               const double ke = k ? k[eidx] : 1.0;
+              // separate multiply and add roundings (no contraction), as in a cell-wise scatter
+#ifdef __CUDA_ARCH__
+              v = __dadd_rn(v, __dmul_rn(__dmul_rn(ke, sc), kref[a * nloc + b]));
+#else
               v += ke * sc * kref[a * nloc + b];
+#endif
             }
         emit(j++, uint32_t(uint64_t(x) + M1 * (uint64_t(y) + M1 * z)), v);
       }
@@ -140,6 +153,24 @@ __global__ void k_fill_sell(Geom g, uint64_t n, const uint32_t* __restrict__ cs,
     col[base + uint64_t(j) * 32] = uint32_t(row);
     val[base + uint64_t(j) * 32] = 0.0;
   }
+}
+
+// implicit-column (stencil) copy of a Q1 level matrix: slot j of row r holds a(r, r + off[j])
+__global__ void k_fill_stencil(Geom g, uint64_t n, const double* __restrict__ k, const double* __restrict__ kref,
+                               double sc, double* val) {
+  const uint64_t row = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  if (row >= n) return;
+  const int S = g.dim == 3 ? 27 : 9;
+  const uint64_t c = row >> 5, t = row & 31;
+  uint32_t rc[3];
+  lat_coords(row, g, rc);
+  row_entries(row, g, k, kref, sc, [&](uint32_t, uint32_t col, double v) {
+    uint32_t cc[3];
+    lat_coords(col, g, cc);
+    int slot = 0;
+    for (int d = g.dim - 1; d >= 0; --d) slot = slot * 3 + (int(cc[d]) - int(rc[d]) + 1);
+    val[(c * S + slot) * 32 + t] = v;
+  });
 }
 
 __global__ void k_mask(Geom g, uint64_t n, uint32_t* mask) {
@@ -442,6 +473,23 @@ static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
     nnz1 += hi - lo + 1;
   }
   S.nnz = nnz1 * nnz1 * (g.dim == 3 ? nnz1 : 1);
+  if (g.p == 1) {
+    // implicit-column copy (all rows padded to the full 3^dim stencil; absent neighbours = 0)
+    DevStencil& St = L.St;
+    St.S = g.dim == 3 ? 27 : 9;
+    St.nchunks = S.nchunks;
+    int j = 0;
+    const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
+    for (int dz = z0; dz <= z1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          St.off[j++] = int32_t((int64_t(dz) * g.M1 + dy) * g.M1 + dx);
+    const uint64_t ns = uint64_t(St.nchunks) * St.S * 32;
+    FB_TRY(dalloc(m, &St.v64, ns));
+    FB_CUDA(cudaMemsetAsync(St.v64, 0, sizeof(double) * ns, m->stream));
+    k_fill_stencil<<<grid_for(n, 128), 128, 0, m->stream>>>(g, n, L.k, m->kref, sc, St.v64);
+    FB_CHECK_LAUNCH();
+  }
   FB_TRY(dalloc(m, &L.mask, (n + 31) / 32));
   k_mask<<<grid_for((n + 31) / 32, 256), 256, 0, m->stream>>>(g, n, L.mask);
   FB_CHECK_LAUNCH();
@@ -520,6 +568,12 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
       std::vector<double> va, tva;
       prol1d(m->degree, gf.M, rp, ci, va);
       transpose1d(gf.M1, gc.M1, rp, ci, va, trp, tci, tva);
+      if (m->degree == 1) {
+        Level& Lf = m->L[i];
+        Lf.q1_transfer = true;
+        Lf.tr.dim = m->dim; Lf.tr.Mf1 = gf.M1; Lf.tr.Mc1 = gc.M1;
+        Lf.tr.nf = Lf.n; Lf.tr.nc = m->L[i + 1].n;
+      }
       st = build_kron(m, m->L[i].P, m->dim, gf.M1, gc.M1, rp, ci, va);
       if (st == FB_OK) st = build_kron(m, m->L[i].R, m->dim, gc.M1, gf.M1, trp, tci, tva);
     }

@@ -3,6 +3,8 @@
 // 16-byte vector accesses where the pointers allow it.
 #include "fb_common.cuh"
 
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -33,6 +35,21 @@ int workspace_get(Workspace** out) {
   }
   *out = g_ws[dev];
   return FB_OK;
+}
+
+bool debug_enabled() {
+  static int on = -1;
+  if (on < 0) { const char* e = std::getenv("FB_DEBUG"); on = (e && e[0] == '1') ? 1 : 0; }
+  return on == 1;
+}
+
+cudaError_t debug_sync(cudaStream_t s, const char* file, int line) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) std::fprintf(stderr, "feat3_b200: %s after the launch at %s:%d\n", cudaGetErrorString(e), file, line);
+  return e;
 }
 
 // ------------------------------------------------------------------ elementwise kernels

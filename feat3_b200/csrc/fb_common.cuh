@@ -20,6 +20,11 @@ inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? FB_OK : FB_ERR
 #define FB_TRY(x) do { int _s = (x); if (_s != FB_OK) return _s; } while (0)
 #define FB_CUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
 
+// FB_DEBUG=1 in the environment: synchronise after every launch of the multigrid driver
+// and report the source line of a failing launch (debugging aid; never on by default)
+bool debug_enabled();
+cudaError_t debug_sync(cudaStream_t s, const char* file, int line);
+
 inline unsigned grid_for(uint64_t n, int threads, int per_thread = 1) {
   uint64_t g = (n + uint64_t(threads) * per_thread - 1) / (uint64_t(threads) * per_thread);
   if (g < 1) g = 1;

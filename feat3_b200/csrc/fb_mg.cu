@@ -22,6 +22,14 @@
 #include <numeric>
 #include <vector>
 
+#undef FB_CHECK_LAUNCH
+#define FB_CHECK_LAUNCH()                                                              \
+  do {                                                                                 \
+    cudaError_t _e = cudaGetLastError();                                               \
+    if (_e == cudaSuccess && fb::debug_enabled()) _e = fb::debug_sync(m->stream, __FILE__, __LINE__); \
+    if (_e != cudaSuccess) return FB_ERR_CUDA;                                         \
+  } while (0)
+
 namespace fb {
 
 static int occupancy_grid(const void* fn, uint64_t work_warps) {
@@ -61,6 +69,30 @@ static int launch_csr(fb_mg* m, const DevCsr& A, bool f32, const XT* x, const Ep
   m->launches++;
   FB_CHECK_LAUNCH();
   return FB_OK;
+}
+
+template<typename VT, typename XT, typename AT, typename Epi, int S>
+static int launch_stencil_S(fb_mg* m, const DevStencil& St, const void* val, float scale, uint32_t rows,
+                            const XT* x, const Epi& epi, double* red_out) {
+  StencilView<S> v;
+  v.rows = rows; v.nchunks = St.nchunks; v.val = val; v.scale = scale;
+  for (int j = 0; j < S; ++j) v.off[j] = St.off[j];
+  constexpr int G = S == 27 ? 9 : S;
+  auto fn = k_stencil<VT, XT, AT, Epi, S, G>;
+  fn<<<occupancy_grid((const void*)fn, St.nchunks), 256, 0, m->stream>>>(v, x, epi, m->ws, m->counter, red_out);
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
+template<typename VT, typename XT, typename AT, typename Epi>
+static int launch_stencil(fb_mg* m, const Level& L, int prec, const XT* x, const Epi& epi, double* red_out) {
+  const DevStencil& St = L.St;
+  const void* val = prec == FB_PREC_F64 ? (const void*)St.v64 : (prec == FB_PREC_F32 ? (const void*)St.v32 : (const void*)St.v16);
+  const float scale = prec == FB_PREC_F16 ? St.scale16 : 1.0f;
+  if (St.S == 27) return launch_stencil_S<VT, XT, AT, Epi, 27>(m, St, val, scale, L.n, x, epi, red_out);
+  if (St.S == 9) return launch_stencil_S<VT, XT, AT, Epi, 9>(m, St, val, scale, L.n, x, epi, red_out);
+  return FB_ERR_UNSUPPORTED;
 }
 
 // ------------------------------------------------------------------ small kernels
@@ -211,19 +243,54 @@ template<> struct Prec<float> {
 };
 
 // dispatch a SELL launch on the value storage of the configured precision
-template<typename T, typename Epi>
-static int sell_T(fb_mg* m, const DevSell& A, const T* x, const Epi& epi, double* red) {
-  if (std::is_same<T, double>::value)
-    return launch_sell<double, double, double, Epi>(m, A, FB_PREC_F64, (const double*)x, epi, red);
-  if (m->cfg.precision == FB_PREC_F16)
-    return launch_sell<__half, float, float, Epi>(m, A, FB_PREC_F16, (const float*)x, epi, red);
-  return launch_sell<float, float, float, Epi>(m, A, FB_PREC_F32, (const float*)x, epi, red);
+static bool use_stencil(const fb_mg* m, const Level& L) {
+  return m->cfg.format == FB_FORMAT_STENCIL && L.St.S > 0;
 }
+
+// level operator A x with an epilogue, on the storage the configuration selects
 template<typename T, typename Epi>
-static int csr_T(fb_mg* m, const DevCsr& A, const T* x, const Epi& epi, double* red) {
-  if (std::is_same<T, double>::value)
-    return launch_csr<double, double, double, Epi>(m, A, false, (const double*)x, epi, red);
-  return launch_csr<float, float, float, Epi>(m, A, true, (const float*)x, epi, red);
+static int spmv_L(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* red) {
+  const bool st = use_stencil(m, L);
+  if constexpr (std::is_same<T, double>::value) {
+    if (st) return launch_stencil<double, double, double, Epi>(m, L, FB_PREC_F64, x, epi, red);
+    return launch_sell<double, double, double, Epi>(m, L.A, FB_PREC_F64, x, epi, red);
+  } else {
+    if (m->cfg.precision == FB_PREC_F16) {
+      if (st) return launch_stencil<__half, float, float, Epi>(m, L, FB_PREC_F16, x, epi, red);
+      return launch_sell<__half, float, float, Epi>(m, L.A, FB_PREC_F16, x, epi, red);
+    }
+    if (st) return launch_stencil<float, float, float, Epi>(m, L, FB_PREC_F32, x, epi, red);
+    return launch_sell<float, float, float, Epi>(m, L.A, FB_PREC_F32, x, epi, red);
+  }
+}
+
+// restriction from level l onto level l+1 (R d), epilogue on the coarse rows
+template<typename T, typename Epi>
+static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
+  const Level& L = m->L[l];
+  if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
+    auto fn = k_rest_q1<T, Epi>;
+    fn<<<occupancy_grid((const void*)fn, L.tr.nc / 32 + 1), 256, 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    return FB_OK;
+  }
+  if constexpr (std::is_same<T, double>::value) return launch_csr<double, double, double, Epi>(m, L.R, false, xf, epi, red);
+  else return launch_csr<float, float, float, Epi>(m, L.R, true, xf, epi, red);
+}
+
+// prolongation from level l+1 onto level l (P x_c), epilogue on the fine rows
+template<typename T, typename Epi>
+static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
+  const Level& L = m->L[l];
+  if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
+    k_prol_q1<T, Epi><<<ew_grid(L.tr.nf), 256, 0, m->stream>>>(L.tr, xc, epi);
+    m->launches++;
+    FB_CHECK_LAUNCH();
+    return FB_OK;
+  }
+  if constexpr (std::is_same<T, double>::value) return launch_csr<double, double, double, Epi>(m, L.P, false, xc, epi, nullptr);
+  else return launch_csr<float, float, float, Epi>(m, L.P, true, xc, epi, nullptr);
 }
 
 // pre-smoothing from zero with rhs b on level l (Richardson(Jacobi), nu steps); `cur` holds
@@ -241,7 +308,7 @@ static int presmooth(fb_mg* m, int l, const T* b, const double* bnorm, bool need
   }
   for (int it = 1; it < m->cfg.nu; ++it) {
     EpiJacobi<T, false> e{cur, b, Prec<T>::invd(L), oth, nullptr, L.mask, bnorm, omega};
-    FB_TRY(sell_T<T>(m, L.A, cur, e, nullptr));
+    FB_TRY(spmv_L<T>(m, L, cur, e, nullptr));
     std::swap(cur, oth);
   }
   *result = cur;
@@ -263,12 +330,12 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     const bool need_s1 = (l == 0) || nu < 2;
     FB_TRY(presmooth<T>(m, l, b, bn, need_s1, &sol[l]));
     EpiDefect<T, false, false> ed{Prec<T>::def(L), b, L.mask, nullptr};
-    FB_TRY(sell_T<T>(m, L.A, sol[l], ed, nullptr));
+    FB_TRY(spmv_L<T>(m, L, sol[l], ed, nullptr));
     const bool coarsest_next = (l + 2 == nl);
     T* s1 = nullptr;
     if (nu >= 2 && (!coarsest_next || m->cfg.coarse == FB_COARSE_SMOOTHER)) s1 = Prec<T>::x(C);
     EpiRestrict<T> er{Prec<T>::rhs(C), s1, Prec<T>::invd(C), C.mask, omega};
-    FB_TRY(csr_T<T>(m, L.R, Prec<T>::def(L), er, &m->sc->lvl[2 * (l + 1)]));
+    FB_TRY(rest_T<T>(m, l, Prec<T>::def(L), er, &m->sc->lvl[2 * (l + 1)]));
   }
   // ---- coarse grid (multigrid.hpp:1524-1587)
   {
@@ -278,7 +345,8 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     const double* bn = (l == 0) ? rhs_top_sumsq : &m->sc->lvl[2 * l];
     switch (m->cfg.coarse) {
       case FB_COARSE_DIRECT: {
-        const T* cinv = std::is_same<T, double>::value ? (const T*)m->cinv64 : (const T*)m->cinv32;
+        const T* cinv;
+        if constexpr (std::is_same<T, double>::value) cinv = m->cinv64; else cinv = m->cinv32;
         k_dense_solve<T><<<grid_for(uint64_t(L.n) * 32, 256), 256, 0, m->stream>>>(Prec<T>::x(L), cinv, b, L.n);
         m->launches++;
         FB_CHECK_LAUNCH();
@@ -304,13 +372,13 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     T* cur = sol[l];
     T* oth = (cur == Prec<T>::x(L)) ? Prec<T>::y(L) : Prec<T>::x(L);
     EpiProlong<T> ep{cur, L.mask};
-    FB_TRY(csr_T<T>(m, L.P, sol[l + 1], ep, nullptr));
+    FB_TRY(prol_T<T>(m, l, sol[l + 1], ep));
     T* s0 = cur;
     double* dn = &m->sc->lvl[2 * l + 1];
     for (int it = 0; it < nu; ++it) {
       if (it == 0) {
         EpiJacobi<T, true> e{cur, b, Prec<T>::invd(L), oth, nullptr, L.mask, nullptr, omega};
-        FB_TRY(sell_T<T>(m, L.A, cur, e, dn));
+        FB_TRY(spmv_L<T>(m, L, cur, e, dn));
         if (nu == 1) {
           k_skip_fix<T><<<ew_grid(L.n), 256, 0, m->stream>>>(oth, s0, dn, L.n);
           m->launches++;
@@ -318,7 +386,7 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
         }
       } else {
         EpiJacobi<T, false> e{cur, b, Prec<T>::invd(L), oth, s0, L.mask, dn, omega};
-        FB_TRY(sell_T<T>(m, L.A, cur, e, nullptr));
+        FB_TRY(spmv_L<T>(m, L, cur, e, nullptr));
       }
       std::swap(cur, oth);
     }
@@ -358,10 +426,10 @@ static int outer_defect(fb_mg* m) {
   Level& L = m->L[0];
   if (m->cfg.precision == FB_PREC_F64) {
     EpiDefect<double, true, false> e{m->r, m->bb, L.mask, nullptr};
-    return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->xb, e, &m->sc->rr);
+    return spmv_L<double>(m, L, (const double*)m->xb, e, &m->sc->rr);
   }
   EpiDefect<double, true, true> e{m->r, m->bb, L.mask, m->r32};
-  return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->xb, e, &m->sc->rr);
+  return spmv_L<double>(m, L, (const double*)m->xb, e, &m->sc->rr);
 }
 
 // z-like output of the preconditioner (FP64 or FP32 buffer)
@@ -398,7 +466,7 @@ static int body(fb_mg* m) {
     m->launches++;
     FB_CHECK_LAUNCH();
     EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
-    FB_TRY((launch_sell<double, double, double>(m, m->L[0].A, FB_PREC_F64, (const double*)m->p, eq, &m->sc->qp)));
+    FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
     if (low) k_pcg_update<true><<<occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
     else     k_pcg_update<false><<<occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
     m->launches++;
@@ -415,8 +483,8 @@ static int body(fb_mg* m) {
 }
 
 static int run_body(fb_mg* m) {
-  if (!m->cfg.use_graphs) return body(m);
-  const int key = m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
+  if (!m->cfg.use_graphs || debug_enabled()) return body(m);
+  const int key = m->cfg.format * 64 + m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
   if (!m->g_body || m->g_body_key != key) {
     if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; }
     cudaGraph_t g = nullptr;
@@ -461,6 +529,29 @@ static int ensure_vectors(fb_mg* m, int prec) {
         FB_TRY(dalloc(m, &L.P.v32, L.P.nnz)); FB_TRY(dalloc(m, &L.R.v32, L.R.nnz));
         k_cvt<float, double><<<ew_grid(L.P.nnz), 256, 0, m->stream>>>(L.P.v32, L.P.v64, L.P.nnz);
         k_cvt<float, double><<<ew_grid(L.R.nnz), 256, 0, m->stream>>>(L.R.v32, L.R.v64, L.R.nnz);
+        FB_CHECK_LAUNCH();
+      }
+      if (L.St.S && prec == FB_PREC_F32 && !L.St.v32) {
+        const uint64_t ns = uint64_t(L.St.nchunks) * L.St.S * 32;
+        FB_TRY(dalloc(m, &L.St.v32, ns));
+        k_cvt<float, double><<<ew_grid(ns), 256, 0, m->stream>>>(L.St.v32, L.St.v64, ns);
+        FB_CHECK_LAUNCH();
+      }
+      if (L.St.S && prec == FB_PREC_F16 && !L.St.v16) {
+        const uint64_t ns = uint64_t(L.St.nchunks) * L.St.S * 32;
+        unsigned long long* dmax = nullptr;
+        FB_TRY(dalloc(m, &dmax, 1));
+        FB_CUDA(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), m->stream));
+        k_absmax<<<ew_grid(ns), 256, 0, m->stream>>>(L.St.v64, ns, dmax);
+        FB_CHECK_LAUNCH();
+        unsigned long long hm = 0;
+        FB_CUDA(cudaMemcpyAsync(&hm, dmax, sizeof(hm), cudaMemcpyDeviceToHost, m->stream));
+        FB_CUDA(cudaStreamSynchronize(m->stream));
+        double amax;
+        std::memcpy(&amax, &hm, sizeof(double));
+        L.St.scale16 = float(amax > 0.0 ? amax / 16384.0 : 1.0);
+        FB_TRY(dalloc(m, &L.St.v16, ns));
+        k_quant16<<<ew_grid(ns), 256, 0, m->stream>>>(L.St.v16, L.St.v64, 1.0 / double(L.St.scale16), ns);
         FB_CHECK_LAUNCH();
       }
       if (prec == FB_PREC_F32 && !L.A.v32) {
@@ -721,12 +812,14 @@ void fb_solver_cfg_default(fb_solver_cfg* c) {
   c->max_iter = 1000;
   c->precision = FB_PREC_F64;
   c->use_graphs = 1;
+  c->format = FB_FORMAT_SELL;
 }
 
 int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (!m || !c) return FB_ERR_INVALID;
   if (c->nu < 1 || c->nu > 64 || c->max_iter < 0 || !(c->tol_rel >= 0.0) ||
-      c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3)
+      c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3 ||
+      c->format < 0 || c->format > 1)
     return FB_ERR_INVALID;
   if (c->coarse == FB_COARSE_PCG) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;
@@ -868,15 +961,15 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
   auto one = [&]() -> int {
     if (!low) {
       double* b = level == 0 ? m->r : L.rhs64;
-      if (which == 0) { EpiJacobi<double, false> e{L.x64, b, L.invd64, L.y64, nullptr, L.mask, nullptr, m->cfg.omega_rich}; return sell_T<double>(m, L.A, L.x64, e, nullptr); }
-      if (which == 1) { EpiDefect<double, false, false> e{L.def64, b, L.mask, nullptr}; return sell_T<double>(m, L.A, L.x64, e, nullptr); }
+      if (which == 0) { EpiJacobi<double, false> e{L.x64, b, L.invd64, L.y64, nullptr, L.mask, nullptr, m->cfg.omega_rich}; return spmv_L<double>(m, L, L.x64, e, nullptr); }
+      if (which == 1) { EpiDefect<double, false, false> e{L.def64, b, L.mask, nullptr}; return spmv_L<double>(m, L, L.x64, e, nullptr); }
       EpiPcgQ<double> e{m->q, m->p, L.mask};
-      return launch_sell<double, double, double>(m, L.A, FB_PREC_F64, (const double*)m->p, e, &m->sc->tmp[0]);
+      return spmv_L<double>(m, L, (const double*)m->p, e, &m->sc->tmp[0]);
     }
     float* b = level == 0 ? m->r32 : L.rhs32;
-    if (which == 0) { EpiJacobi<float, false> e{L.x32, b, L.invd32, L.y32, nullptr, L.mask, nullptr, float(m->cfg.omega_rich)}; return sell_T<float>(m, L.A, L.x32, e, nullptr); }
+    if (which == 0) { EpiJacobi<float, false> e{L.x32, b, L.invd32, L.y32, nullptr, L.mask, nullptr, float(m->cfg.omega_rich)}; return spmv_L<float>(m, L, L.x32, e, nullptr); }
     EpiDefect<float, false, false> e{L.def32, b, L.mask, nullptr};
-    return sell_T<float>(m, L.A, L.x32, e, nullptr);
+    return spmv_L<float>(m, L, L.x32, e, nullptr);
   };
   int st = one();  // warm-up
   if (st == FB_OK) st = cuda_status(cudaEventRecord(m->ev0, m->stream));

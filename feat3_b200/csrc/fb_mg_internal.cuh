@@ -48,8 +48,21 @@ struct DevCsr {
   }
 };
 
+struct DevStencil {
+  int S = 0;                 // stencil size (0 = not available on this level)
+  int32_t off[27] = {0};     // neighbour offsets in ascending order
+  uint32_t nchunks = 0;
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+  __half* v16 = nullptr;
+  float scale16 = 1.0f;
+};
+
 struct Level {
   uint32_t n = 0;
+  DevStencil St;         // implicit-column copy of A (structured Q1 only)
+  bool q1_transfer = false;
+  Q1Transfer tr;         // matrix-free transfer between this level and the next coarser one
   DevSell A;
   DevCsr P, R;           // P: this level <- next coarser level; R: next coarser <- this
   double* diag = nullptr;

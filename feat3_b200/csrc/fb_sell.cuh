@@ -220,3 +220,130 @@ __global__ void __launch_bounds__(256) k_csr_epi(CsrView A, const XT* __restrict
 }
 
 }  // namespace fb
+
+namespace fb {
+
+// ------------------------------------------------------------------ stencil SELL
+// SELL-32 with implicit column indices for lattice matrices whose every row has the
+// same stencil of S neighbour offsets (Q1 on a structured grid: S = 9 in 2D, 27 in 3D).
+// Slot j of row r holds a(r, r + off[j]) (0 where the neighbour does not exist), stored
+// chunk-major like SELL: val[(c*S + j)*32 + lane]. No column-index stream is read: the
+// neighbour index is computed, so the x loads are independent of any other load.
+template<int S>
+struct StencilView {
+  uint32_t rows, nchunks;
+  const void* val;
+  float scale;
+  int32_t off[S];
+};
+
+template<typename VT, typename XT, typename AT, typename Epi, int S, int G>
+__global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __restrict__ x, Epi epi,
+                                                 double* ws, unsigned* counter, double* red_out) {
+  __shared__ double sh[8];
+  const int lane = threadIdx.x & 31;
+  const uint32_t wpb = blockDim.x >> 5;
+  const VT* __restrict__ val = static_cast<const VT*>(A.val);
+  const int64_t last = int64_t(A.rows) - 1;
+  double acc = 0.0;
+  for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < A.nchunks; c += gridDim.x * wpb) {
+    const int64_t row = int64_t(c) * 32 + lane;
+    const VT* vp = val + size_t(c) * S * 32 + lane;
+    AT sum = AT(0);
+#pragma unroll
+    for (int j0 = 0; j0 < S; j0 += G) {
+      AT vv[G], xx[G];
+#pragma unroll
+      for (int u = 0; u < G; ++u) {
+        if (j0 + u < S) {
+          int64_t col = row + A.off[j0 + u];
+          col = col < 0 ? 0 : (col > last ? last : col);
+          vv[u] = AT(ld_stream(vp + (j0 + u) * 32));
+          xx[u] = AT(__ldg(x + col));
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < G; ++u)
+        if (j0 + u < S) sum += vv[u] * xx[u];
+    }
+    if (row <= last) {
+      if (sizeof(VT) == 2) sum *= AT(A.scale);
+      acc += epi(uint32_t(row), sum);
+    }
+  }
+  if (Epi::kReduce) {
+    const double blk = block_sum<256>(acc, sh);
+    reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+// ------------------------------------------------------------------ matrix-free Q1 transfers
+// Nested Q1 interpolation on lexicographic lattices: fine coordinate X takes coarse X/2
+// (weight 1) when even, (X-1)/2 and (X+1)/2 (weight 1/2 each) when odd; P is the tensor
+// product, R = P^T. Terms are summed in ascending coarse (resp. fine) index order.
+struct Q1Transfer {
+  int dim;
+  uint32_t Mf1, Mc1;   // lattice points per side, fine and coarse
+  uint32_t nf, nc;
+};
+
+template<typename T, typename Epi>
+__global__ void k_prol_q1(Q1Transfer g, const T* __restrict__ xc, Epi epi) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.nf; i += gridDim.x * blockDim.x) {
+    const uint32_t X = i % g.Mf1, Y = (i / g.Mf1) % g.Mf1, Z = g.dim == 3 ? i / (g.Mf1 * g.Mf1) : 0u;
+    const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
+    const uint32_t cz0 = Z >> 1, cz1 = (Z + 1) >> 1;
+    const T wx = (X & 1) ? T(0.5) : T(1), wy = (Y & 1) ? T(0.5) : T(1), wz = (Z & 1) ? T(0.5) : T(1);
+    T s = T(0);
+    const int nz = (g.dim == 3 && (Z & 1)) ? 2 : 1, ny = (Y & 1) ? 2 : 1, nx = (X & 1) ? 2 : 1;
+    for (int a = 0; a < nz; ++a) {
+      const uint32_t cz = a ? cz1 : cz0;
+      for (int b = 0; b < ny; ++b) {
+        const uint32_t cy = b ? cy1 : cy0;
+        const size_t base = (size_t(cz) * g.Mc1 + cy) * g.Mc1;
+        for (int d = 0; d < nx; ++d) {
+          const uint32_t cx = d ? cx1 : cx0;
+          s += (wx * wy * wz) * xc[base + cx];
+        }
+      }
+    }
+    epi(i, s);
+  }
+}
+
+template<typename T, typename Epi>
+__global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restrict__ xf, Epi epi,
+                                                 double* ws, unsigned* counter, double* red_out) {
+  __shared__ double sh[8];
+  double acc = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.nc; i += gridDim.x * blockDim.x) {
+    const int X = int(i % g.Mc1), Y = int((i / g.Mc1) % g.Mc1), Z = g.dim == 3 ? int(i / (g.Mc1 * g.Mc1)) : 0;
+    const int F = int(g.Mf1) - 1;
+    T s = T(0);
+    const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
+    for (int dz = z0; dz <= z1; ++dz) {
+      const int fz = 2 * Z + dz;
+      if (fz < 0 || fz > (g.dim == 3 ? F : 0)) continue;
+      const T wz = dz ? T(0.5) : T(1);
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int fy = 2 * Y + dy;
+        if (fy < 0 || fy > F) continue;
+        const T wy = dy ? T(0.5) : T(1);
+        const size_t base = (size_t(fz) * g.Mf1 + fy) * g.Mf1;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int fx = 2 * X + dx;
+          if (fx < 0 || fx > F) continue;
+          const T wx = dx ? T(0.5) : T(1);
+          s += (wx * wy * wz) * xf[base + fx];
+        }
+      }
+    }
+    acc += epi(i, s);
+  }
+  if (Epi::kReduce) {
+    const double blk = block_sum<256>(acc, sh);
+    reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+}  // namespace fb

@@ -20,6 +20,7 @@ STATUS = {0: "undefined", 1: "progress", 2: "success", 3: "aborted", 4: "diverge
 OUTER = {"pcg": 0, "richardson": 1}
 COARSE = {"direct": 0, "pcg": 1, "smoother": 2, "none": 3}
 PRECISION = {"f64": 0, "f32": 1, "f16": 2}
+FORMAT = {"sell": 0, "stencil": 1}
 RHS = {"sine": 0, "one": 1, "expbubble": 2}
 
 
@@ -99,9 +100,9 @@ class MultiGrid:
 
     # ---------------------------------------------------------------- configuration
     def configure(self, outer="pcg", nu=4, omega_jac=0.5, omega_rich=1.0, omega_outer=1.0, coarse="direct",
-                  tol=1e-8, max_iter=1000, precision="f64", graphs=True):
+                  tol=1e-8, max_iter=1000, precision="f64", graphs=True, format="sell"):
         cfg = _lib.SolverCfg(OUTER[outer], nu, omega_jac, omega_rich, omega_outer, COARSE[coarse], tol, max_iter,
-                             PRECISION[precision], 1 if graphs else 0)
+                             PRECISION[precision], 1 if graphs else 0, FORMAT[format])
         _lib.check("fb_mg_configure", _lib.load().fb_mg_configure(self.h, C.byref(cfg)))
         self.cfg = cfg
         return self

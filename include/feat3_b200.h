@@ -177,6 +177,14 @@ FB_API void fb_mg_destroy(fb_mg* mg);
 #define FB_PREC_F64 0
 #define FB_PREC_F32 1
 #define FB_PREC_F16 2
+/* level-matrix storage of the V-cycle and the outer solver:
+ *   FB_FORMAT_SELL    SELL-C-sigma with 32-bit column indices and CSR transfer matrices
+ *                     (what a hierarchy handed over by FEAT3 uses);
+ *   FB_FORMAT_STENCIL on structured Q1 hierarchies: SELL-32 with implicit stencil columns
+ *                     (no index stream) and matrix-free Q1 interpolation/restriction;
+ *                     other hierarchies fall back to FB_FORMAT_SELL level by level. */
+#define FB_FORMAT_SELL 0
+#define FB_FORMAT_STENCIL 1
 typedef struct fb_solver_cfg {
   int outer;
   int nu;
@@ -188,6 +196,7 @@ typedef struct fb_solver_cfg {
   int max_iter;
   int precision;
   int use_graphs;     /* capture the per-iteration launch sequence in a CUDA graph */
+  int format;         /* FB_FORMAT_SELL or FB_FORMAT_STENCIL */
 } fb_solver_cfg;
 FB_API void fb_solver_cfg_default(fb_solver_cfg* cfg);
 FB_API int fb_mg_configure(fb_mg* mg, const fb_solver_cfg* cfg);

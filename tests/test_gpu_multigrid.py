@@ -37,8 +37,8 @@ CASES = [
 
 
 @pytest.mark.parametrize("case", CASES, ids=[f"d{c[0]}q{c[1]}L{c[2]}-{c[4]}-k{c[5]}-nu{c[6]}-{c[8]}" for c in CASES])
-@pytest.mark.parametrize("graphs", [True, False])
-def test_structured_pcg_matches_oracle(case, graphs):
+@pytest.mark.parametrize("graphs,fmt", [(True, "sell"), (False, "sell"), (True, "stencil"), (False, "stencil")])
+def test_structured_pcg_matches_oracle(case, graphs, fmt):
     from feat3_b200.solver import MultiGrid
     dim, deg, lvl, lmin, rhs, ks, nu, wj, coarse = case
     k = None if ks is None else lognormal_k(dim, lvl, ks, seed=lvl)
@@ -46,7 +46,7 @@ def test_structured_pcg_matches_oracle(case, graphs):
     b = H.rhs(rhs)
     ref = H.solve(b, nu=nu, omega_jac=wj, coarse=coarse)
     mg = MultiGrid.structured(dim, deg, lvl, lmin, k)
-    mg.configure(nu=nu, omega_jac=wj, coarse=coarse, graphs=graphs)
+    mg.configure(nu=nu, omega_jac=wj, coarse=coarse, graphs=graphs, format=fmt)
     bg = mg.assemble_rhs(rhs)
     np.testing.assert_allclose(bg.cpu().numpy(), b, rtol=1e-12, atol=1e-15 * np.abs(b).max())
     res = mg.solve(torch.tensor(b).cuda())
@@ -93,14 +93,15 @@ def test_csr_hierarchy_dropin(sigma):
 
 
 @pytest.mark.parametrize("outer", ["richardson", "pcg"])
-def test_richardson_outer(outer):
+@pytest.mark.parametrize("graphs", [False, True])
+def test_richardson_outer(outer, graphs):
     from feat3_b200.solver import MultiGrid
     H = po.Hierarchy(2, 1, 7, 1)
     b = H.rhs("sine")
     kw = dict(nu=4, omega_jac=1.0, omega_rich=0.8, coarse="direct")
     ref = H.solve(b, solver=outer, **kw)
     mg = MultiGrid.structured(2, 1, 7, 1)
-    mg.configure(outer=outer, **kw)
+    mg.configure(outer=outer, graphs=graphs, **kw)
     res = mg.solve(torch.tensor(b).cuda())
     assert res["iters"] == ref["iters"]
     assert relerr(res["u"].cpu().numpy(), ref["u"]) <= TOL_U
@@ -108,14 +109,15 @@ def test_richardson_outer(outer):
 
 @pytest.mark.parametrize("prec", ["f32", "f16"])
 @pytest.mark.parametrize("outer", ["richardson", "pcg"])
-def test_mixed_precision_error(prec, outer):
+@pytest.mark.parametrize("fmt", ["sell", "stencil"])
+def test_mixed_precision_error(prec, outer, fmt):
     from feat3_b200.solver import MultiGrid
     k = lognormal_k(3, 5, 1.0, seed=5)
     H = po.Hierarchy(3, 1, 5, 1, k)
     b = H.rhs("one")
     ref = H.solve(b, nu=2, tol=1e-12)
     mg = MultiGrid.structured(3, 1, 5, 1, k)
-    mg.configure(nu=2, precision=prec, outer=outer)
+    mg.configure(nu=2, precision=prec, outer=outer, format=fmt)
     res = mg.solve(torch.tensor(b).cuda())
     assert res["status"] == "success"
     assert res["hist"][-1] <= 1e-8 * res["hist"][0]
@@ -145,12 +147,13 @@ def test_zero_rhs_and_nan_status():
     assert r["status"] == "aborted"
 
 
-def test_vcycle_matches_oracle():
+@pytest.mark.parametrize("fmt", ["sell", "stencil"])
+def test_vcycle_matches_oracle(fmt):
     from feat3_b200.solver import MultiGrid
     H = po.Hierarchy(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11))
     d = H.rhs("one")
     ref = H.vcycle(d, nu=2)
-    mg = MultiGrid.structured(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11)).configure(nu=2)
+    mg = MultiGrid.structured(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11)).configure(nu=2, format=fmt)
     cor = mg.vcycle(torch.tensor(d).cuda()).cpu().numpy()
     assert relerr(cor, ref) <= 1e-13
 
