@@ -229,6 +229,23 @@ def native_arm(args):
     clocks = clk.stop()
     umx = rmx["u"]
     err = float(torch.linalg.norm(umx - u64) / torch.linalg.norm(u64))
+    # --- one adjoint gradient solve on the same hierarchy (transposed MG-PCG + element gradient)
+    u_target = (0.9 * umx).contiguous()
+    adj = {}
+    for prec in ("f16", "f64"):
+        mg.configure(precision=prec, format="stencil", **common)
+        mg.adjoint_grad(umx, u_target)  # warm-up
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        lam, grad, ainfo = mg.adjoint_grad(umx, u_target)
+        torch.cuda.synchronize()
+        adj[prec] = {"time_s": time.perf_counter() - t0, "solve_s": ainfo["solve_ms"] / 1e3, "iters": ainfo["iters"],
+                     "status": ainfo["status"], "grad_norm": float(torch.linalg.norm(grad))}
+        adj[prec + "_grad"] = grad
+    adj_err = float(torch.linalg.norm(adj["f16_grad"] - adj["f64_grad"]) / torch.linalg.norm(adj["f64_grad"]))
+    adjoint = {"mixed": adj["f16"], "fp64": adj["f64"], "grad_rel_diff_mixed_vs_fp64": adj_err,
+               "objective": "J = 1/2 ||u - u_t||^2, u_t = 0.9 u"}
     # --- end to end through the host-buffer entry point
     re2e, te2e, _, _, _ = run_form("f16", max(2, args.steps // 2), 1, host=True, fmt="stencil")
 
@@ -283,6 +300,7 @@ def native_arm(args):
             "roofline": {"bound": "hbm", "achieved": dom["GBps"], "peak": peak, "unit": "GB/s",
                          "frac": dom["GBps"] / peak, "traffic": None, "kernel": "k_stencil<__half,float,float,EpiJacobi,27> finest level (FP16 values, implicit columns)",
                          "kernels": rf, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650"},
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
             "gpu_launches": lmx,

@@ -136,21 +136,26 @@ __global__ void k_rowlen(Geom g, uint64_t n, uint32_t* rl, uint32_t* cl) {
   if ((threadIdx.x & 31) == 0 && row < n) cl[row >> 5] = mx;
 }
 
-__global__ void k_fill_sell(Geom g, uint64_t n, const uint32_t* __restrict__ cs, const uint32_t* __restrict__ cl,
-                            const double* __restrict__ k, const double* __restrict__ kref, double sc,
-                            uint32_t* col, double* val) {
+// one thread per SELL slot row (nchunks*32 threads): rows beyond n in the last chunk get
+// padding too, because the SELL kernels load every lane's column and gather x with it
+__global__ void k_fill_sell(Geom g, uint64_t n, uint32_t nchunks, const uint32_t* __restrict__ cs,
+                            const uint32_t* __restrict__ cl, const double* __restrict__ k,
+                            const double* __restrict__ kref, double sc, uint32_t* col, double* val) {
   const uint64_t row = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
-  if (row >= n) return;
+  if (row >= uint64_t(nchunks) * 32) return;
   const uint32_t ch = uint32_t(row >> 5), t = uint32_t(row & 31);
   const uint64_t base = uint64_t(cs[ch]) + t;
   uint32_t used = 0;
-  row_entries(row, g, k, kref, sc, [&](uint32_t j, uint32_t c, double v) {
-    col[base + uint64_t(j) * 32] = c;
-    val[base + uint64_t(j) * 32] = v;
-    used = j + 1;
-  });
+  if (row < n) {
+    row_entries(row, g, k, kref, sc, [&](uint32_t j, uint32_t c, double v) {
+      col[base + uint64_t(j) * 32] = c;
+      val[base + uint64_t(j) * 32] = v;
+      used = j + 1;
+    });
+  }
+  const uint32_t pad_col = row < n ? uint32_t(row) : uint32_t(n - 1);
   for (uint32_t j = used; j < cl[ch]; ++j) {
-    col[base + uint64_t(j) * 32] = uint32_t(row);
+    col[base + uint64_t(j) * 32] = pad_col;
     val[base + uint64_t(j) * 32] = 0.0;
   }
 }
@@ -460,10 +465,12 @@ static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
   }
   cs[S.nchunks] = uint32_t(acc);
   S.nent = acc;
-  FB_CUDA(cudaMemcpy(S.cs, cs.data(), sizeof(uint32_t) * cs.size(), cudaMemcpyHostToDevice));
+  FB_CUDA(cudaMemcpyAsync(S.cs, cs.data(), sizeof(uint32_t) * cs.size(), cudaMemcpyHostToDevice, m->stream));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_TRY(dalloc(m, &S.col, S.nent));
   FB_TRY(dalloc(m, &S.v64, S.nent));
-  k_fill_sell<<<grid_for(n, 128), 128, 0, m->stream>>>(g, n, S.cs, S.cl, L.k, m->kref, sc, S.col, S.v64);
+  k_fill_sell<<<grid_for(uint64_t(S.nchunks) * 32, 128), 128, 0, m->stream>>>(g, n, S.nchunks, S.cs, S.cl, L.k, m->kref,
+                                                                             sc, S.col, S.v64);
   FB_CHECK_LAUNCH();
   // true nonzeros: sum of row lengths (closed form per direction)
   uint64_t nnz1 = 0;
@@ -547,7 +554,10 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
         st = dalloc(m, &L.k, L.ne);
         if (st != FB_OK) break;
         if (i == 0) {
-          if (cudaMemcpy(L.k, d->k, sizeof(double) * L.ne, d->k_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice) != cudaSuccess) st = FB_ERR_CUDA;
+          // stream-ordered copy; a device-side k must be complete before this call (the caller's stream)
+          if (cudaMemcpyAsync(L.k, d->k, sizeof(double) * L.ne, d->k_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                              m->stream) != cudaSuccess ||
+              cudaStreamSynchronize(m->stream) != cudaSuccess) st = FB_ERR_CUDA;
         } else {
           k_coarsen_k<<<grid_for(L.ne, 256), 256, 0, m->stream>>>(m->dim, g.N, m->L[i - 1].k, L.k);
           if (cudaGetLastError() != cudaSuccess) st = FB_ERR_CUDA;
@@ -585,7 +595,8 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
       std::vector<double> kc;
       if (C.k) {
         kc.resize(C.ne);
-        if (cudaMemcpy(kc.data(), C.k, sizeof(double) * C.ne, cudaMemcpyDeviceToHost) != cudaSuccess) { st = FB_ERR_CUDA; break; }
+        if (cudaMemcpyAsync(kc.data(), C.k, sizeof(double) * C.ne, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
+            cudaStreamSynchronize(m->stream) != cudaSuccess) { st = FB_ERR_CUDA; break; }
       }
       HostCsr h;
       h.rows = h.cols = C.n;
@@ -604,6 +615,7 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
         if (bd) filt.push_back(uint32_t(r));
       }
       if (C.n <= 4096) st = build_coarse_inverse(m, h, filt);
+      if (st == FB_OK) st = upload_coarse_csr(m, h);
     }
     if (st != FB_OK) break;
     st = finish_levels(m);

@@ -30,7 +30,9 @@ int workspace_get(Workspace** out) {
       delete w;
       return FB_ERR_ALLOC;
     }
-    if (cudaMemset(w->counter, 0, sizeof(unsigned) * 8) != cudaSuccess) return FB_ERR_CUDA;
+    // one-time initialisation, complete before any stream (blocking or not) can use the counter
+    if (cudaMemset(w->counter, 0, sizeof(unsigned) * 8) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+      return FB_ERR_CUDA;
     g_ws[dev] = w;
   }
   *out = g_ws[dev];
@@ -50,6 +52,10 @@ cudaError_t debug_sync(cudaStream_t s, const char* file, int line) {
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) std::fprintf(stderr, "feat3_b200: %s after the launch at %s:%d\n", cudaGetErrorString(e), file, line);
   return e;
+}
+
+void debug_report(cudaError_t e, const char* what, const char* file, int line) {
+  std::fprintf(stderr, "feat3_b200: %s returned %s at %s:%d\n", what, cudaGetErrorString(e), file, line);
 }
 
 // ------------------------------------------------------------------ elementwise kernels

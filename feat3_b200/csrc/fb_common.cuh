@@ -14,16 +14,25 @@ constexpr int kWarp = 32;
 constexpr int kRedBlocks = 4 * kSMs; // reduction grid: 4 resident CTAs per SM
 constexpr int kRedThreads = 256;
 
-// map a CUDA error onto the C-ABI status
-inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? FB_OK : FB_ERR_CUDA; }
-#define FB_CHECK_LAUNCH() do { cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
-#define FB_TRY(x) do { int _s = (x); if (_s != FB_OK) return _s; } while (0)
-#define FB_CUDA(x) do { cudaError_t _e = (x); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
-
 // FB_DEBUG=1 in the environment: synchronise after every launch of the multigrid driver
 // and report the source line of a failing launch (debugging aid; never on by default)
 bool debug_enabled();
 cudaError_t debug_sync(cudaStream_t s, const char* file, int line);
+void debug_report(cudaError_t e, const char* what, const char* file, int line);
+
+// map a CUDA error onto the C-ABI status
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? FB_OK : FB_ERR_CUDA; }
+#define FB_CHECK_LAUNCH() do { cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)
+#define FB_TRY(x) do { int _s = (x); if (_s != FB_OK) return _s; } while (0)
+#define FB_CUDA(x)                                                                       \
+  do {                                                                                   \
+    cudaError_t _e = (x);                                                                \
+    if (_e != cudaSuccess) {                                                             \
+      if (fb::debug_enabled()) fb::debug_report(_e, #x, __FILE__, __LINE__);             \
+      return FB_ERR_CUDA;                                                                \
+    }                                                                                    \
+  } while (0)
+
 
 inline unsigned grid_for(uint64_t n, int threads, int per_thread = 1) {
   uint64_t g = (n + uint64_t(threads) * per_thread - 1) / (uint64_t(threads) * per_thread);
@@ -60,6 +69,21 @@ __device__ __forceinline__ double block_sum(double v, double* sh /* THREADS/32 *
   return r;  // valid in thread 0
 }
 
+// block sum for 2D/3D blocks: `tid` = flattened thread index; result valid in tid 0
+template<int THREADS>
+__device__ __forceinline__ double block_sum_tid(double v, double* sh, uint32_t tid) {
+  v = warp_sum(v);
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = (lane < THREADS / 32) ? sh[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;
+}
+
 // Finish a reduction: thread 0 of every CTA passes its CTA partial. Returns true in the one
 // thread (of the last CTA) that wrote `*out` (the final sum, optionally transformed).
 // The partials buffer and counter live in `ws`/`counter`.
@@ -85,6 +109,36 @@ __device__ __forceinline__ bool reduce_finish(double blk, double* ws, unsigned* 
     *counter = 0u;
   }
   return threadIdx.x == 0;
+}
+
+// the same finish for 2D/3D grids: `bid` = linear block index, `nblk` = number of blocks
+template<int THREADS>
+__device__ __forceinline__ bool reduce_finish_nd(double blk, double* ws, unsigned* counter, double* out,
+                                                 double* sh, uint32_t bid, uint32_t nblk) {
+  __shared__ bool am_last;
+  const uint32_t tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  if (tid == 0) {
+    ws[bid] = blk;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    am_last = (t == nblk - 1);
+  }
+  __syncthreads();
+  if (!am_last) return false;
+  __threadfence();
+  double v = 0.0;
+  for (uint32_t i = tid; i < nblk; i += THREADS) v += ((volatile double*)ws)[i];
+  // block_sum indexes by threadIdx.x: flatten is equivalent for 1D-flattened warps
+  v = warp_sum(v);
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    double r = (lane < THREADS / 32) ? sh[lane] : 0.0;
+    r = warp_sum(r);
+    if (lane == 0) { *out = r; *counter = 0u; }
+  }
+  return tid == 0;
 }
 
 // per-device library workspace for the stand-alone reductions of the operator C-ABI

@@ -18,6 +18,8 @@
 #include "fb_mg_internal.cuh"
 
 #include <algorithm>
+#include <cstdio>
+#include <initializer_list>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -43,10 +45,27 @@ static int occupancy_grid(const void* fn, uint64_t work_warps) {
 }
 
 // ------------------------------------------------------------------ launch helpers
+// debugging aid (FB_DEBUG=1): report pointers that are not device memory of this context
+static void debug_check_ptrs(const char* what, std::initializer_list<const void*> ptrs) {
+  int i = 0;
+  for (const void* p : ptrs) {
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (p && (e != cudaSuccess || at.type != cudaMemoryTypeDevice))
+      std::fprintf(stderr, "feat3_b200: %s pointer #%d = %p is not device memory (err %d type %d)\n", what, i, p,
+                   int(e), e == cudaSuccess ? int(at.type) : -1);
+    cudaGetLastError();
+    ++i;
+  }
+}
+
 template<typename VT, typename XT, typename AT, typename Epi>
 static int launch_sell(fb_mg* m, const DevSell& A, int prec, const XT* x, const Epi& epi, double* red_out) {
   auto fn = k_sell<VT, XT, AT, Epi, 8>;
   const int grid = occupancy_grid((const void*)fn, A.nchunks);
+  if (debug_enabled())
+    debug_check_ptrs("k_sell", {A.cs, A.cl, A.col, A.view(prec).val, (const void*)x, (const void*)m->ws,
+                                (const void*)m->counter, (const void*)red_out, (const void*)A.perm});
   fn<<<grid, 256, 0, m->stream>>>(A.view(prec), x, epi, m->ws, m->counter, red_out);
   m->launches++;
   FB_CHECK_LAUNCH();
@@ -85,9 +104,30 @@ static int launch_stencil_S(fb_mg* m, const DevStencil& St, const void* val, flo
   return FB_OK;
 }
 
+template<typename VT, typename Epi, int S>
+static int launch_stencil_packed_S(fb_mg* m, const DevStencil& St, const void* val, float scale, uint32_t rows,
+                                   const float* x, const Epi& epi, double* red_out) {
+  StencilView<S> v;
+  v.rows = rows; v.nchunks = St.nchunks; v.val = val; v.scale = scale;
+  for (int j = 0; j < S; ++j) v.off[j] = St.off[j];
+  auto fn = k_stencil_packed<VT, Epi, S>;
+  fn<<<occupancy_grid((const void*)fn, St.nchunks), 256, 0, m->stream>>>(v, x, epi, m->ws, m->counter, red_out);
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
 template<typename VT, typename XT, typename AT, typename Epi>
 static int launch_stencil(fb_mg* m, const Level& L, int prec, const XT* x, const Epi& epi, double* red_out) {
   const DevStencil& St = L.St;
+  if constexpr (!std::is_same<VT, double>::value) {
+    // 2- and 4-byte values use the packed layout (8-byte loads per lane)
+    const float scale = prec == FB_PREC_F16 ? St.scale16 : 1.0f;
+    const void* pv = prec == FB_PREC_F16 ? (const void*)St.v16 : (const void*)St.v32;
+    if (St.S == 27) return launch_stencil_packed_S<VT, Epi, 27>(m, St, pv, scale, L.n, x, epi, red_out);
+    if (St.S == 9) return launch_stencil_packed_S<VT, Epi, 9>(m, St, pv, scale, L.n, x, epi, red_out);
+    return FB_ERR_UNSUPPORTED;
+  }
   const void* val = prec == FB_PREC_F64 ? (const void*)St.v64 : (prec == FB_PREC_F32 ? (const void*)St.v32 : (const void*)St.v16);
   const float scale = prec == FB_PREC_F16 ? St.scale16 : 1.0f;
   if (St.S == 27) return launch_stencil_S<VT, XT, AT, Epi, 27>(m, St, val, scale, L.n, x, epi, red_out);
@@ -130,6 +170,61 @@ template<typename T>
 __global__ void k_copy_masked(T* x, const T* __restrict__ b, const uint32_t* mask, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     x[i] = masked(mask, i) ? T(0) : b[i];
+}
+
+// Unpreconditioned CG on the coarsest level in one CTA, with the reference's default settings
+// (Solver::new_pcg(matrix, filter), used as coarse solver by tutorial_05_multigrid.cpp:420-436):
+// x = 0, r = b, stop on tol_rel = sqrt(eps) relative to ||r0||, divergence, non-finite
+// defects or max_iter = 100 (pcg.hpp:139-287, iterative.hpp:216-235, 744-832).
+template<typename T, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __restrict__ b, T* x, T* r, T* p, T* q,
+                                                        const uint32_t* mask, uint32_t n, int max_iter) {
+  __shared__ double sh[THREADS / 32];
+  __shared__ double bc;
+  const T* val = static_cast<const T*>(A.val);
+  auto dot = [&](const T* u, const T* v) -> double {
+    double a = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) a += double(u[i]) * double(v[i]);
+    __syncthreads();
+    const double s = block_sum<THREADS>(a, sh);
+    if (threadIdx.x == 0) bc = s;
+    __syncthreads();
+    return bc;
+  };
+  const double e = double(eps_of<T>());
+  const double tol_rel = sqrt(e), div_rel = 1.0 / e, big = 1.0 / (e * e);
+  for (uint32_t i = threadIdx.x; i < n; i += THREADS) { r[i] = b[i]; x[i] = T(0); }
+  __syncthreads();
+  const double d0 = sqrt(dot(r, r));
+  if (!isfinite(d0) || d0 <= e * e) return;
+  for (uint32_t i = threadIdx.x; i < n; i += THREADS) p[i] = masked(mask, i) ? T(0) : r[i];
+  __syncthreads();
+  double gamma = dot(r, p);
+  for (int it = 1; it <= max_iter; ++it) {
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+      T s = T(0);
+      for (uint32_t k = A.rp[i]; k < A.rp[i + 1]; ++k) s += val[k] * p[A.col[k]];
+      q[i] = masked(mask, i) ? T(0) : s;
+    }
+    __syncthreads();
+    const T alpha = T(gamma / dot(q, p));
+    const bool upd = fabs(double(alpha)) >= e;
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) {
+      if (upd) { x[i] = alpha * p[i] + x[i]; r[i] = (-alpha) * q[i] + r[i]; }
+    }
+    __syncthreads();
+    const double dc = sqrt(dot(r, r));
+    if (!isfinite(dc) || dc > big || dc > div_rel * d0) return;
+    if (dc <= big && dc <= tol_rel * d0) return;
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) q[i] = masked(mask, i) ? T(0) : r[i];  // z
+    __syncthreads();
+    const double g2 = gamma;
+    gamma = dot(r, q);
+    const T beta = T(gamma / g2);
+    const bool ub = fabs(double(beta)) >= e;
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) p[i] = ub ? beta * p[i] + q[i] : q[i];
+    __syncthreads();
+  }
 }
 
 // PCG update: alpha = gamma / qp; x += alpha p; r -= alpha q; ||r||^2 (+ FP32 copy of r)
@@ -269,8 +364,8 @@ template<typename T, typename Epi>
 static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
   const Level& L = m->L[l];
   if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
-    auto fn = k_rest_q1<T, Epi>;
-    fn<<<occupancy_grid((const void*)fn, L.tr.nc / 32 + 1), 256, 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
+    const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, L.tr.dim == 3 ? L.tr.Mc1 : 1);
+    k_rest_q1<T, Epi><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
     m->launches++;
     FB_CHECK_LAUNCH();
     return FB_OK;
@@ -284,7 +379,8 @@ template<typename T, typename Epi>
 static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
   const Level& L = m->L[l];
   if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
-    k_prol_q1<T, Epi><<<ew_grid(L.tr.nf), 256, 0, m->stream>>>(L.tr, xc, epi);
+    const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, L.tr.dim == 3 ? L.tr.Mf1 : 1);
+    k_prol_q1<T, Epi><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xc, epi);
     m->launches++;
     FB_CHECK_LAUNCH();
     return FB_OK;
@@ -356,6 +452,17 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
       case FB_COARSE_SMOOTHER:
         FB_TRY(presmooth<T>(m, l, b, bn, l == 0 || nu < 2, &sol[l]));
         break;
+      case FB_COARSE_PCG: {
+        T* w;
+        if constexpr (std::is_same<T, double>::value) w = m->cg64; else w = m->cg32;
+        const uint32_t nc = L.n;
+        k_coarse_cg<T, 512><<<1, 512, 0, m->stream>>>(m->coarse_csr.view(!std::is_same<T, double>::value), b,
+                                                      Prec<T>::x(L), w, w + nc, w + 2 * uint64_t(nc), L.mask, nc, 100);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+      }
       case FB_COARSE_NONE:
       default:
         k_copy_masked<T><<<ew_grid(L.n), 256, 0, m->stream>>>(Prec<T>::x(L), b, L.mask, L.n);
@@ -532,9 +639,9 @@ static int ensure_vectors(fb_mg* m, int prec) {
         FB_CHECK_LAUNCH();
       }
       if (L.St.S && prec == FB_PREC_F32 && !L.St.v32) {
-        const uint64_t ns = uint64_t(L.St.nchunks) * L.St.S * 32;
-        FB_TRY(dalloc(m, &L.St.v32, ns));
-        k_cvt<float, double><<<ew_grid(ns), 256, 0, m->stream>>>(L.St.v32, L.St.v64, ns);
+        const uint64_t np = uint64_t(L.St.nchunks) * ((L.St.S + 1) / 2) * 32 * 2;
+        FB_TRY(dalloc(m, &L.St.v32, np));
+        k_stencil_pack<float><<<ew_grid(np), 256, 0, m->stream>>>(L.St.v32, L.St.v64, L.St.nchunks, L.St.S, 1.0);
         FB_CHECK_LAUNCH();
       }
       if (L.St.S && prec == FB_PREC_F16 && !L.St.v16) {
@@ -550,8 +657,10 @@ static int ensure_vectors(fb_mg* m, int prec) {
         double amax;
         std::memcpy(&amax, &hm, sizeof(double));
         L.St.scale16 = float(amax > 0.0 ? amax / 16384.0 : 1.0);
-        FB_TRY(dalloc(m, &L.St.v16, ns));
-        k_quant16<<<ew_grid(ns), 256, 0, m->stream>>>(L.St.v16, L.St.v64, 1.0 / double(L.St.scale16), ns);
+        const uint64_t np = uint64_t(L.St.nchunks) * ((L.St.S + 3) / 4) * 32 * 4;
+        FB_TRY(dalloc(m, &L.St.v16, np));
+        k_stencil_pack<__half><<<ew_grid(np), 256, 0, m->stream>>>(L.St.v16, L.St.v64, L.St.nchunks, L.St.S,
+                                                                     1.0 / double(L.St.scale16));
         FB_CHECK_LAUNCH();
       }
       if (prec == FB_PREC_F32 && !L.A.v32) {
@@ -577,6 +686,16 @@ static int ensure_vectors(fb_mg* m, int prec) {
         k_quant16<<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v16, L.A.v64, 1.0 / double(L.A.scale16), L.A.nent);
         FB_CHECK_LAUNCH();
       }
+    }
+  }
+  if (m->coarse_csr.rp) {
+    const uint64_t nc = m->coarse_csr.rows;
+    if (!low && !m->cg64) FB_TRY(dalloc(m, &m->cg64, 3 * nc));
+    if (low && !m->cg32) FB_TRY(dalloc(m, &m->cg32, 3 * nc));
+    if (low && !m->coarse_csr.v32) {
+      FB_TRY(dalloc(m, &m->coarse_csr.v32, m->coarse_csr.nnz));
+      k_cvt<float, double><<<ew_grid(m->coarse_csr.nnz), 256, 0, m->stream>>>(m->coarse_csr.v32, m->coarse_csr.v64, m->coarse_csr.nnz);
+      FB_CHECK_LAUNCH();
     }
   }
   if (low && m->cinv64 && !m->cinv32) {
@@ -661,6 +780,11 @@ int upload_csr(fb_mg* m, DevCsr& D, const HostCsr& A) {
   return FB_OK;
 }
 
+int upload_coarse_csr(fb_mg* m, const HostCsr& A) {
+  if (A.rows > 65536) return FB_OK;  // the single-CTA coarse CG is offered for small coarse levels only
+  return upload_csr(m, m->coarse_csr, A);
+}
+
 int upload_filter(fb_mg* m, Level& L, const std::vector<uint32_t>& f) {
   std::vector<uint32_t> mask((L.n + 31) / 32, 0u);
   for (uint32_t i : f) {
@@ -713,10 +837,11 @@ int common_init(fb_mg* m) {
   FB_CUDA(cudaGetDevice(&m->device));
   FB_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   FB_TRY(dalloc(m, &m->sc, 1));
-  FB_CUDA(cudaMemset(m->sc, 0, sizeof(DevScalars)));
+  FB_CUDA(cudaMemsetAsync(m->sc, 0, sizeof(DevScalars), m->stream));
   FB_TRY(dalloc(m, &m->ws, 8192));
   FB_TRY(dalloc(m, &m->counter, 4));
-  FB_CUDA(cudaMemset(m->counter, 0, 4 * sizeof(unsigned)));
+  FB_CUDA(cudaMemsetAsync(m->counter, 0, 4 * sizeof(unsigned), m->stream));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
   FB_CUDA(cudaEventCreate(&m->ev0));
   FB_CUDA(cudaEventCreate(&m->ev1));
@@ -739,6 +864,12 @@ __global__ void k_diag_sell(double* d, SellView A) {
 }
 
 int finish_levels(fb_mg* m) {
+  // reduction partials: one per CTA of the largest reducing launch (3D-grid restriction)
+  uint64_t need = 8192;
+  for (auto& L : m->L)
+    if (L.q1_transfer)
+      need = std::max<uint64_t>(need, uint64_t((L.tr.Mc1 + 31) / 32) * ((L.tr.Mc1 + 7) / 8) * (L.tr.dim == 3 ? L.tr.Mc1 : 1));
+  if (need > 8192) FB_TRY(dalloc(m, &m->ws, need));
   for (auto& L : m->L) {
     if (!L.diag) FB_TRY(dalloc(m, &L.diag, L.n));
     k_diag_sell<<<grid_for(L.n, 256), 256, 0, m->stream>>>(L.diag, L.A.view(FB_PREC_F64));
@@ -821,7 +952,7 @@ int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
       c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3 ||
       c->format < 0 || c->format > 1)
     return FB_ERR_INVALID;
-  if (c->coarse == FB_COARSE_PCG) return FB_ERR_UNSUPPORTED;
+  if (c->coarse == FB_COARSE_PCG && !m->coarse_csr.rp) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;
   FB_CUDA(cudaSetDevice(m->device));
   const bool omega_changed = !m->configured || c->omega_jac != m->cfg.omega_jac;
@@ -870,6 +1001,7 @@ int fb_mg_create_csr(fb_mg** out, int nl, const fb_csr_host* A, const fb_csr_hos
     if (l + 1 == nl) { coarseA = std::move(h); coarseF = f; }
   }
   if (st == FB_OK) st = build_coarse_inverse(m, coarseA, coarseF);
+  if (st == FB_OK) st = upload_coarse_csr(m, coarseA);
   if (st == FB_OK) st = finish_levels(m);
   if (st != FB_OK) { fb_mg_destroy(m); return st; }
   *out = m;

@@ -95,6 +95,10 @@ struct fb_mg {
   int nloc = 0;
   double* kref = nullptr;        // unit-coefficient element matrix on [-1,1]^d (device)
   std::vector<double> kref_h;
+  // coarse level as CSR (for the single-CTA CG coarse solver) and its work vectors
+  fb::DevCsr coarse_csr;
+  double *cg64 = nullptr;        // 3 vectors (r, p, q) of the coarse size
+  float* cg32 = nullptr;
   // coarse direct solver
   uint32_t nc = 0;
   double* cinv64 = nullptr;
@@ -132,16 +136,22 @@ int dalloc(fb_mg* m, T** p, uint64_t n) {
   m->allocs.push_back(*p);
   return FB_OK;
 }
+// Upload a host array. The copy is issued on the hierarchy's own stream (a non-blocking
+// stream: it is NOT ordered after the legacy default stream), so every kernel launched on that
+// stream afterwards sees the data; the host array may be released when this returns.
 template<typename T>
 int dupload(fb_mg* m, T** p, const T* h, uint64_t n) {
   int st = dalloc(m, p, n);
   if (st != FB_OK) return st;
-  if (n && cudaMemcpy(*p, h, sizeof(T) * n, cudaMemcpyHostToDevice) != cudaSuccess) return FB_ERR_CUDA;
+  if (n && (cudaMemcpyAsync(*p, h, sizeof(T) * n, cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+            cudaStreamSynchronize(m->stream) != cudaSuccess))
+    return FB_ERR_CUDA;
   return FB_OK;
 }
 int common_init(fb_mg* m);
 int finish_levels(fb_mg* m);
 int build_coarse_inverse(fb_mg* m, const HostCsr& A, const std::vector<uint32_t>& filt);
+int upload_coarse_csr(fb_mg* m, const HostCsr& A);
 int upload_sell(fb_mg* m, DevSell& S, const HostCsr& A, int sigma);
 int upload_csr(fb_mg* m, DevCsr& D, const HostCsr& A);
 int upload_filter(fb_mg* m, Level& L, const std::vector<uint32_t>& f);

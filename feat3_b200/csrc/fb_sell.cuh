@@ -244,27 +244,46 @@ __global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __r
   const int lane = threadIdx.x & 31;
   const uint32_t wpb = blockDim.x >> 5;
   const VT* __restrict__ val = static_cast<const VT*>(A.val);
-  const int64_t last = int64_t(A.rows) - 1;
+  const int32_t last = int32_t(A.rows) - 1;  // rows < 2^31 (checked when the hierarchy is built)
   double acc = 0.0;
   for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < A.nchunks; c += gridDim.x * wpb) {
-    const int64_t row = int64_t(c) * 32 + lane;
+    const int32_t row0 = int32_t(c) * 32;
+    const int32_t row = row0 + lane;
     const VT* vp = val + size_t(c) * S * 32 + lane;
+    // warp-uniform: every neighbour of every row of the chunk lies inside the vector
+    const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
     AT sum = AT(0);
+    if (inside) {
+      const XT* xr = x + row;
 #pragma unroll
-    for (int j0 = 0; j0 < S; j0 += G) {
-      AT vv[G], xx[G];
+      for (int j0 = 0; j0 < S; j0 += G) {
+        AT vv[G], xx[G];
 #pragma unroll
-      for (int u = 0; u < G; ++u) {
-        if (j0 + u < S) {
-          int64_t col = row + A.off[j0 + u];
-          col = col < 0 ? 0 : (col > last ? last : col);
-          vv[u] = AT(ld_stream(vp + (j0 + u) * 32));
-          xx[u] = AT(__ldg(x + col));
-        }
+        for (int u = 0; u < G; ++u)
+          if (j0 + u < S) {
+            vv[u] = AT(ld_stream(vp + (j0 + u) * 32));
+            xx[u] = AT(__ldg(xr + A.off[j0 + u]));
+          }
+#pragma unroll
+        for (int u = 0; u < G; ++u)
+          if (j0 + u < S) sum += vv[u] * xx[u];
       }
+    } else {
 #pragma unroll
-      for (int u = 0; u < G; ++u)
-        if (j0 + u < S) sum += vv[u] * xx[u];
+      for (int j0 = 0; j0 < S; j0 += G) {
+        AT vv[G], xx[G];
+#pragma unroll
+        for (int u = 0; u < G; ++u)
+          if (j0 + u < S) {
+            int32_t col = row + A.off[j0 + u];
+            col = col < 0 ? 0 : (col > last ? last : col);
+            vv[u] = AT(ld_stream(vp + (j0 + u) * 32));
+            xx[u] = AT(__ldg(x + col));
+          }
+#pragma unroll
+        for (int u = 0; u < G; ++u)
+          if (j0 + u < S) sum += vv[u] * xx[u];
+      }
     }
     if (row <= last) {
       if (sizeof(VT) == 2) sum *= AT(A.scale);
@@ -274,6 +293,83 @@ __global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __r
   if (Epi::kReduce) {
     const double blk = block_sum<256>(acc, sh);
     reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+// Packed stencil storage for 2- and 4-byte values: every lane reads 8 bytes per load, i.e.
+// W = 8 / sizeof(value) consecutive slots of its row: val[((c*G + g)*32 + lane)*W + e] holds
+// slot j = g*W + e (G = ceil(S/W); slots j >= S hold 0). A warp load is 256 contiguous bytes.
+template<typename VT> struct Pack8;
+template<> struct Pack8<__half> {
+  static constexpr int W = 4;
+  __device__ __forceinline__ static void ld(const __half* p, float* v) {
+    const uint2 w = __ldcs(reinterpret_cast<const uint2*>(p));
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+};
+template<> struct Pack8<float> {
+  static constexpr int W = 2;
+  __device__ __forceinline__ static void ld(const float* p, float* v) {
+    const float2 w = __ldcs(reinterpret_cast<const float2*>(p));
+    v[0] = w.x; v[1] = w.y;
+  }
+};
+
+template<typename VT, typename Epi, int S>
+__global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, const float* __restrict__ x, Epi epi,
+                                                           double* ws, unsigned* counter, double* red_out) {
+  constexpr int W = Pack8<VT>::W;
+  constexpr int G = (S + W - 1) / W;
+  __shared__ double sh[8];
+  const int lane = threadIdx.x & 31;
+  const uint32_t wpb = blockDim.x >> 5;
+  const VT* __restrict__ val = static_cast<const VT*>(A.val);
+  const int32_t last = int32_t(A.rows) - 1;
+  double acc = 0.0;
+  for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < A.nchunks; c += gridDim.x * wpb) {
+    const int32_t row0 = int32_t(c) * 32;
+    const int32_t row = row0 + lane;
+    const VT* vp = val + (size_t(c) * G * 32 + lane) * W;
+    const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
+    float sum = 0.0f;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      float v[W];
+      Pack8<VT>::ld(vp + g * 32 * W, v);
+#pragma unroll
+      for (int e = 0; e < W; ++e) {
+        const int j = g * W + e;
+        if (j < S) {
+          int32_t col = row + A.off[j];
+          if (!inside) col = col < 0 ? 0 : (col > last ? last : col);
+          sum += v[e] * __ldg(x + col);
+        }
+      }
+    }
+    if (row <= last) {
+      if (sizeof(VT) == 2) sum *= A.scale;
+      acc += epi(uint32_t(row), sum);
+    }
+  }
+  if (Epi::kReduce) {
+    const double blk = block_sum<256>(acc, sh);
+    reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+// FP64 stencil array [c][j][lane] -> packed 8-byte layout of VT (scaled by inv for FP16)
+template<typename VT>
+__global__ void k_stencil_pack(VT* dst, const double* __restrict__ src, uint32_t nchunks, int S, double inv) {
+  constexpr int W = Pack8<VT>::W;
+  const int G = (S + W - 1) / W;
+  const uint64_t total = uint64_t(nchunks) * G * 32 * W;
+  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t e = i % W, lane = (i / W) % 32, g = (i / (32 * W)) % G, c = i / (uint64_t(32) * W * G);
+    const uint64_t j = g * W + e;
+    const double v = j < uint64_t(S) ? src[(c * S + j) * 32 + lane] * inv : 0.0;
+    dst[i] = VT(v);
   }
 }
 
@@ -287,40 +383,40 @@ struct Q1Transfer {
   uint32_t nf, nc;
 };
 
+// launched on a (ceil(M1/32), ceil(M1/8), M1 or 1) grid of 32x8 blocks: no index division
 template<typename T, typename Epi>
-__global__ void k_prol_q1(Q1Transfer g, const T* __restrict__ xc, Epi epi) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.nf; i += gridDim.x * blockDim.x) {
-    const uint32_t X = i % g.Mf1, Y = (i / g.Mf1) % g.Mf1, Z = g.dim == 3 ? i / (g.Mf1 * g.Mf1) : 0u;
-    const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
-    const uint32_t cz0 = Z >> 1, cz1 = (Z + 1) >> 1;
-    const T wx = (X & 1) ? T(0.5) : T(1), wy = (Y & 1) ? T(0.5) : T(1), wz = (Z & 1) ? T(0.5) : T(1);
-    T s = T(0);
-    const int nz = (g.dim == 3 && (Z & 1)) ? 2 : 1, ny = (Y & 1) ? 2 : 1, nx = (X & 1) ? 2 : 1;
-    for (int a = 0; a < nz; ++a) {
-      const uint32_t cz = a ? cz1 : cz0;
-      for (int b = 0; b < ny; ++b) {
-        const uint32_t cy = b ? cy1 : cy0;
-        const size_t base = (size_t(cz) * g.Mc1 + cy) * g.Mc1;
-        for (int d = 0; d < nx; ++d) {
-          const uint32_t cx = d ? cx1 : cx0;
-          s += (wx * wy * wz) * xc[base + cx];
-        }
-      }
+__global__ void __launch_bounds__(256) k_prol_q1(Q1Transfer g, const T* __restrict__ xc, Epi epi) {
+  const uint32_t X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+  if (X >= g.Mf1 || Y >= g.Mf1) return;
+  const uint32_t i = X + g.Mf1 * (Y + g.Mf1 * Z);
+  const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
+  const uint32_t cz0 = Z >> 1, cz1 = (Z + 1) >> 1;
+  const T w = ((X & 1) ? T(0.5) : T(1)) * ((Y & 1) ? T(0.5) : T(1)) * ((Z & 1) ? T(0.5) : T(1));
+  const int nz = (Z & 1) ? 2 : 1, ny = (Y & 1) ? 2 : 1, nx = (X & 1) ? 2 : 1;
+  T s = T(0);
+  for (int a = 0; a < nz; ++a) {
+    const uint32_t cz = a ? cz1 : cz0;
+    for (int b = 0; b < ny; ++b) {
+      const uint32_t cy = b ? cy1 : cy0;
+      const T* row = xc + (size_t(cz) * g.Mc1 + cy) * g.Mc1;
+      for (int d = 0; d < nx; ++d) s += w * row[d ? cx1 : cx0];
     }
-    epi(i, s);
   }
+  epi(i, s);
 }
 
+// launched on a (ceil(Mc1/32), ceil(Mc1/8), Mc1 or 1) grid of 32x8 blocks
 template<typename T, typename Epi>
 __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restrict__ xf, Epi epi,
                                                  double* ws, unsigned* counter, double* red_out) {
   __shared__ double sh[8];
+  const int X = int(blockIdx.x * 32 + threadIdx.x), Y = int(blockIdx.y * 8 + threadIdx.y), Z = int(blockIdx.z);
   double acc = 0.0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.nc; i += gridDim.x * blockDim.x) {
-    const int X = int(i % g.Mc1), Y = int((i / g.Mc1) % g.Mc1), Z = g.dim == 3 ? int(i / (g.Mc1 * g.Mc1)) : 0;
+  if (X < int(g.Mc1) && Y < int(g.Mc1)) {
+    const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
     const int F = int(g.Mf1) - 1;
-    T s = T(0);
     const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
+    T s = T(0);
     for (int dz = z0; dz <= z1; ++dz) {
       const int fz = 2 * Z + dz;
       if (fz < 0 || fz > (g.dim == 3 ? F : 0)) continue;
@@ -329,20 +425,23 @@ __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restri
         const int fy = 2 * Y + dy;
         if (fy < 0 || fy > F) continue;
         const T wy = dy ? T(0.5) : T(1);
-        const size_t base = (size_t(fz) * g.Mf1 + fy) * g.Mf1;
+        const T* row = xf + (size_t(fz) * g.Mf1 + fy) * g.Mf1;
         for (int dx = -1; dx <= 1; ++dx) {
           const int fx = 2 * X + dx;
           if (fx < 0 || fx > F) continue;
           const T wx = dx ? T(0.5) : T(1);
-          s += (wx * wy * wz) * xf[base + fx];
+          s += (wx * wy * wz) * row[fx];
         }
       }
     }
-    acc += epi(i, s);
+    acc = epi(i, s);
   }
   if (Epi::kReduce) {
-    const double blk = block_sum<256>(acc, sh);
-    reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+    const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const double blk = block_sum_tid<256>(acc, sh, tid);
+    const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
+    const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
   }
 }
 

@@ -24,8 +24,10 @@ FORMAT = {"sell": 0, "stencil": 1}
 RHS = {"sine": 0, "one": 1, "expbubble": 2}
 
 
-def _stream_sync():
-    torch.cuda.synchronize()
+def _torch_sync():
+    """The library runs on its own non-blocking stream: finish torch's pending work on the
+    tensors handed over (and on memory torch may recycle) before every call."""
+    torch.cuda.current_stream().synchronize()
 
 
 class MultiGrid:
@@ -46,6 +48,7 @@ class MultiGrid:
             if isinstance(k, torch.Tensor) and k.is_cuda:
                 karr = k.contiguous().to(torch.float64)
                 desc.k, desc.k_on_device = karr.data_ptr(), 1
+                _torch_sync()
             else:
                 karr = np.ascontiguousarray(np.asarray(k, dtype=np.float64))
                 desc.k = karr.ctypes.data
@@ -127,7 +130,8 @@ class MultiGrid:
 
     # ---------------------------------------------------------------- work
     def assemble_rhs(self, kind="sine"):
-        b = torch.zeros(self.ndofs(), dtype=torch.float64, device="cuda")
+        b = torch.empty(self.ndofs(), dtype=torch.float64, device="cuda")
+        _torch_sync()
         _lib.call("fb_mg_assemble_rhs", self.h, RHS[kind], b.data_ptr())
         return b
 
@@ -145,7 +149,7 @@ class MultiGrid:
             sol = torch.zeros_like(rhs)
         hist = np.zeros(self.cfg.max_iter + 1) if record else None
         info = _lib.SolveInfo()
-        torch.cuda.current_stream().synchronize()
+        _torch_sync()
         _lib.call("fb_mg_solve", self.h, rhs.data_ptr(), sol.data_ptr(),
                   None if hist is None else hist.ctypes.data, C.byref(info))
         out = self._info(info, hist)
@@ -168,12 +172,14 @@ class MultiGrid:
 
     def vcycle(self, d):
         cor = torch.empty_like(d)
+        _torch_sync()
         _lib.call("fb_mg_vcycle", self.h, d.data_ptr(), cor.data_ptr())
         return cor
 
     def element_grad(self, u, lam):
         ne = (1 << self.level) ** self.dim
         g = torch.empty(ne, dtype=torch.float64, device="cuda")
+        _torch_sync()
         _lib.call("fb_mg_element_grad", self.h, u.data_ptr(), lam.data_ptr(), g.data_ptr())
         return g
 
@@ -183,6 +189,7 @@ class MultiGrid:
         lam = torch.empty_like(u)
         g = torch.empty(ne, dtype=torch.float64, device="cuda")
         info = _lib.SolveInfo()
+        _torch_sync()
         _lib.call("fb_mg_adjoint_grad", self.h, u.data_ptr(), u_target.data_ptr(), lam.data_ptr(), g.data_ptr(),
                   C.byref(info))
         return lam, g, self._info(info, None)
