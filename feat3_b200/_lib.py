@@ -14,8 +14,9 @@ from . import build as _build
 HERE = os.path.dirname(os.path.abspath(__file__))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "feat3_b200.h")
 
-FB_OK, FB_ERR_INVALID, FB_ERR_CUDA, FB_ERR_ALLOC, FB_ERR_UNSUPPORTED, FB_ERR_NOT_READY = range(6)
-ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported", 5: "not ready"}
+FB_OK, FB_ERR_INVALID, FB_ERR_CUDA, FB_ERR_ALLOC, FB_ERR_UNSUPPORTED, FB_ERR_NOT_READY, FB_ERR_TOO_LARGE = range(7)
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported", 5: "not ready",
+          6: "exceeds a fixed capacity"}
 
 
 class FeatError(RuntimeError):
@@ -58,6 +59,7 @@ _SIGS = {
     "fb_dot_f32": [vp, vp, u64, vp, vp],
     "fb_dot_f64_sync": [vp, vp, u64, vp, vp],
     "fb_dot_f32_sync": [vp, vp, u64, vp, vp],
+    "fb_dot_f64_noalloc": [vp, vp, u64, vp, vp],
     "fb_norm2_f64": [vp, u64, vp, vp],
     "fb_norm2_f32": [vp, u64, vp, vp],
     "fb_norm2_f64_sync": [vp, u64, vp, vp],

@@ -31,6 +31,7 @@ extern "C" {
 #define FB_ERR_ALLOC 3        /* device or pinned allocation failed */
 #define FB_ERR_UNSUPPORTED 4  /* combination not implemented */
 #define FB_ERR_NOT_READY 5    /* object not initialised */
+#define FB_ERR_TOO_LARGE 6    /* request exceeds a fixed capacity of the entry point */
 
 #if defined(__GNUC__)
 #define FB_API __attribute__((visibility("default")))
@@ -78,6 +79,20 @@ FB_API int fb_dot_f32(const float* x, const float* y, uint64_t n, double* result
 /* same, returning the value to the host (synchronises `stream`), as the reference's value() */
 FB_API int fb_dot_f64_sync(const double* x, const double* y, uint64_t n, double* host_result, fb_stream_t stream);
 FB_API int fb_dot_f32_sync(const float* x, const float* y, uint64_t n, double* host_result, fb_stream_t stream);
+
+/* No counterpart in the reference: a variant of fb_dot_f64 that allocates nothing, for callers
+ * that cannot call cudaMalloc (an external allocator owns all device memory, or allocation is
+ * forbidden after start-up). Its partial sums live in a fixed device array inside the library
+ * (FB_NOALLOC_DOT_MAX_CTAS doubles plus a counter, 32 KiB on every GPU that loads the library,
+ * held until exit), so n is limited to FB_NOALLOC_DOT_MAX_N elements; larger n returns
+ * FB_ERR_TOO_LARGE. The first call on each device looks up the array's device address; make
+ * that first call before any stream capture. All calls share the one array: calls that
+ * overlap on the GPU (concurrent streams) race and must be serialised by the caller.
+ * *result (device) = x . y, as fb_dot_f64. */
+#define FB_NOALLOC_DOT_MAX_CTAS 4096
+#define FB_NOALLOC_DOT_ELEMS_PER_CTA 16384ull
+#define FB_NOALLOC_DOT_MAX_N (4096ull * 16384ull)
+FB_API int fb_dot_f64_noalloc(const double* x, const double* y, uint64_t n, double* result, fb_stream_t stream);
 
 /* *result (device) = ||x||_2. Replaces Arch::Norm2<Mem::CUDA>::value (norm.cu:24-60). */
 FB_API int fb_norm2_f64(const double* x, uint64_t n, double* result, fb_stream_t stream);
