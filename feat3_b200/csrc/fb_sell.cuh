@@ -383,7 +383,10 @@ struct Q1Transfer {
   uint32_t nf, nc;
 };
 
-// launched on a (ceil(M1/32), ceil(M1/8), M1 or 1) grid of 32x8 blocks: no index division
+// launched on a (ceil(M1/32), ceil(M1/8), M1 or 1) grid of 32x8 blocks: no index division.
+// Every fine point reads the 2^dim coarse corners around it with independent loads; for an
+// even coordinate both corners coincide and the second carries weight 0, so the terms and
+// their order are those of the CSR row (plus exact zeros).
 template<typename T, typename Epi>
 __global__ void __launch_bounds__(256) k_prol_q1(Q1Transfer g, const T* __restrict__ xc, Epi epi) {
   const uint32_t X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
@@ -392,20 +395,32 @@ __global__ void __launch_bounds__(256) k_prol_q1(Q1Transfer g, const T* __restri
   const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
   const uint32_t cz0 = Z >> 1, cz1 = (Z + 1) >> 1;
   const T w = ((X & 1) ? T(0.5) : T(1)) * ((Y & 1) ? T(0.5) : T(1)) * ((Z & 1) ? T(0.5) : T(1));
-  const int nz = (Z & 1) ? 2 : 1, ny = (Y & 1) ? 2 : 1, nx = (X & 1) ? 2 : 1;
+  const T wx1 = (X & 1) ? w : T(0), wy1 = (Y & 1) ? T(1) : T(0), wz1 = (Z & 1) ? T(1) : T(0);
+  const size_t r00 = (size_t(cz0) * g.Mc1 + cy0) * g.Mc1, r01 = (size_t(cz0) * g.Mc1 + cy1) * g.Mc1;
+  T v[8];
+  v[0] = xc[r00 + cx0]; v[1] = xc[r00 + cx1];
+  v[2] = xc[r01 + cx0]; v[3] = xc[r01 + cx1];
+  if (g.dim == 3) {
+    const size_t r10 = (size_t(cz1) * g.Mc1 + cy0) * g.Mc1, r11 = (size_t(cz1) * g.Mc1 + cy1) * g.Mc1;
+    v[4] = xc[r10 + cx0]; v[5] = xc[r10 + cx1];
+    v[6] = xc[r11 + cx0]; v[7] = xc[r11 + cx1];
+  }
   T s = T(0);
-  for (int a = 0; a < nz; ++a) {
-    const uint32_t cz = a ? cz1 : cz0;
-    for (int b = 0; b < ny; ++b) {
-      const uint32_t cy = b ? cy1 : cy0;
-      const T* row = xc + (size_t(cz) * g.Mc1 + cy) * g.Mc1;
-      for (int d = 0; d < nx; ++d) s += w * row[d ? cx1 : cx0];
-    }
+  s += w * v[0];
+  s += wx1 * v[1];
+  s += (wy1 * w) * v[2];
+  s += (wy1 * wx1) * v[3];
+  if (g.dim == 3) {
+    s += (wz1 * w) * v[4];
+    s += (wz1 * wx1) * v[5];
+    s += (wz1 * wy1 * w) * v[6];
+    s += (wz1 * wy1 * wx1) * v[7];
   }
   epi(i, s);
 }
 
-// launched on a (ceil(Mc1/32), ceil(Mc1/8), Mc1 or 1) grid of 32x8 blocks
+// launched on a (ceil(Mc1/32), ceil(Mc1/8), Mc1 or 1) grid of 32x8 blocks; the 3^dim fine
+// neighbours are read with independent loads (indices clamped, weight 0 outside the lattice)
 template<typename T, typename Epi>
 __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restrict__ xf, Epi epi,
                                                  double* ws, unsigned* counter, double* red_out) {
@@ -415,25 +430,36 @@ __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restri
   if (X < int(g.Mc1) && Y < int(g.Mc1)) {
     const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
     const int F = int(g.Mf1) - 1;
-    const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
-    T s = T(0);
-    for (int dz = z0; dz <= z1; ++dz) {
-      const int fz = 2 * Z + dz;
-      if (fz < 0 || fz > (g.dim == 3 ? F : 0)) continue;
-      const T wz = dz ? T(0.5) : T(1);
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int fy = 2 * Y + dy;
-        if (fy < 0 || fy > F) continue;
-        const T wy = dy ? T(0.5) : T(1);
-        const T* row = xf + (size_t(fz) * g.Mf1 + fy) * g.Mf1;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int fx = 2 * X + dx;
-          if (fx < 0 || fx > F) continue;
-          const T wx = dx ? T(0.5) : T(1);
-          s += (wx * wy * wz) * row[fx];
-        }
-      }
+    const int Fz = g.dim == 3 ? F : 0;
+    int fx[3], fy[3], fz[3];
+    T wx[3], wy[3], wz[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int ox = 2 * X + d - 1, oy = 2 * Y + d - 1, oz = 2 * Z + d - 1;
+      const T wd = d == 1 ? T(1) : T(0.5);
+      wx[d] = (ox < 0 || ox > F) ? T(0) : wd;
+      wy[d] = (oy < 0 || oy > F) ? T(0) : wd;
+      wz[d] = (g.dim == 3) ? ((oz < 0 || oz > Fz) ? T(0) : wd) : (d == 1 ? T(1) : T(0));
+      fx[d] = ox < 0 ? 0 : (ox > F ? F : ox);
+      fy[d] = oy < 0 ? 0 : (oy > F ? F : oy);
+      fz[d] = oz < 0 ? 0 : (oz > Fz ? Fz : oz);
     }
+    T v[27];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const T* row = xf + (size_t(fz[a]) * g.Mf1 + fy[b]) * g.Mf1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[(a * 3 + b) * 3 + c] = (g.dim == 3 || a == 1) ? row[fx[c]] : T(0);
+      }
+    T s = T(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) s += (wx[c] * wy[b] * wz[a]) * v[(a * 3 + b) * 3 + c];
     acc = epi(i, s);
   }
   if (Epi::kReduce) {
