@@ -317,6 +317,28 @@ template<> struct Pack8<float> {
   }
 };
 
+// x gathers: the offsets come in runs of three (dx = -1, 0, +1) around each (dy, dz) line
+// centre, so on interior chunks each run is one coalesced load of x[b + lane] plus one
+// two-lane load of the halo (x[b-1] for lane 0, x[b+32] for lane 31) and two shuffles,
+// instead of three 128-byte loads: a third of the L2->SM traffic of the gathers.
+template<int S>
+__device__ __forceinline__ void gather_runs(const float* __restrict__ x, const int32_t* off, int32_t row0, int lane,
+                                            float* xv) {
+#pragma unroll
+  for (int r = 0; r < S / 3; ++r) {
+    const int32_t b = row0 + off[3 * r + 1];  // centre of the run
+    const float c = __ldg(x + b + lane);
+    float e = 0.0f;
+    if (lane == 0) e = __ldg(x + b - 1);
+    else if (lane == 31) e = __ldg(x + b + 32);
+    const float lft = __shfl_up_sync(0xffffffffu, c, 1);
+    const float rgt = __shfl_down_sync(0xffffffffu, c, 1);
+    xv[3 * r + 0] = lane == 0 ? e : lft;
+    xv[3 * r + 1] = c;
+    xv[3 * r + 2] = lane == 31 ? e : rgt;
+  }
+}
+
 template<typename VT, typename Epi, int S>
 __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, const float* __restrict__ x, Epi epi,
                                                            double* ws, unsigned* counter, double* red_out) {
@@ -333,6 +355,17 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
     const int32_t row = row0 + lane;
     const VT* vp = val + (size_t(c) * G * 32 + lane) * W;
     const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
+    float xv[S];
+    if (inside) {
+      gather_runs<S>(x, A.off, row0, lane, xv);
+    } else {
+#pragma unroll
+      for (int j = 0; j < S; ++j) {
+        int32_t col = row + A.off[j];
+        col = col < 0 ? 0 : (col > last ? last : col);
+        xv[j] = __ldg(x + col);
+      }
+    }
     float sum = 0.0f;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -341,11 +374,7 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
 #pragma unroll
       for (int e = 0; e < W; ++e) {
         const int j = g * W + e;
-        if (j < S) {
-          int32_t col = row + A.off[j];
-          if (!inside) col = col < 0 ? 0 : (col > last ? last : col);
-          sum += v[e] * __ldg(x + col);
-        }
+        if (j < S) sum += v[e] * xv[j];
       }
     }
     if (row <= last) {

@@ -156,7 +156,9 @@ def test_adjoint_gradient_finite_differences(precision):
     1/2 sum (u+ - u-)(u+ + u- - 2 u_t). To keep the FP64 round-off of the two solves out of
     the difference, u+ - u- is obtained from the exact identity
         A(g+hd) (u+ - u-) = (A(g-hd) - A(g+hd)) u-,   A(g-hd) - A(g+hd) = A(-2 k sinh(h d)),
-    solved with the same solver. Tolerance 1e-6 relative."""
+    solved with the FP64 solver. The gradient under test comes from solves in `precision`
+    (the mixed form stops at 1e-12, its outer FP64 PCG's attainable accuracy with an FP16/FP32
+    V-cycle). Tolerance 1e-6 relative."""
     from feat3_b200.lafem import DenseVector, SparseMatrixCSR
     from feat3_b200.solver import MultiGrid
     from oracle import pyoracle as po
@@ -164,12 +166,12 @@ def test_adjoint_gradient_finite_differences(precision):
     lvl = int(fx["level"])
     g0 = np.log(fx["k"])
     target = torch.tensor(fx["target"]).cuda()
-    kw = dict(nu=2, omega_jac=0.5, coarse="direct", tol=1e-14, max_iter=100, precision=precision)
+    kw = dict(nu=2, omega_jac=0.5, coarse="direct", tol=1e-14, max_iter=100, precision="f64")
 
-    def hierarchy(g):
-        return MultiGrid.structured(2, 1, lvl, 1, np.exp(g)).configure(**kw)
+    def hierarchy(g, **over):
+        return MultiGrid.structured(2, 1, lvl, 1, np.exp(g)).configure(**{**kw, **over})
 
-    mg = hierarchy(g0)
+    mg = hierarchy(g0, precision=precision, tol=1e-14 if precision == "f64" else 1e-12)
     u = mg.solve(mg.assemble_rhs("one"))["u"]
     _, gk, _ = mg.adjoint_grad(u, target)
     grad_g = gk.cpu().numpy() * np.exp(g0)
