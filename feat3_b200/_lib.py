@@ -14,9 +14,10 @@ from . import build as _build
 HERE = os.path.dirname(os.path.abspath(__file__))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "feat3_b200.h")
 
-FB_OK, FB_ERR_INVALID, FB_ERR_CUDA, FB_ERR_ALLOC, FB_ERR_UNSUPPORTED, FB_ERR_NOT_READY, FB_ERR_TOO_LARGE = range(7)
+(FB_OK, FB_ERR_INVALID, FB_ERR_CUDA, FB_ERR_ALLOC, FB_ERR_UNSUPPORTED, FB_ERR_NOT_READY, FB_ERR_TOO_LARGE,
+ FB_ERR_TIMEOUT) = range(8)
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported", 5: "not ready",
-          6: "exceeds a fixed capacity"}
+          6: "exceeds a fixed capacity", 7: "bounded wait in a kernel expired"}
 
 
 class FeatError(RuntimeError):

@@ -194,6 +194,11 @@ __global__ void k_mask(Geom g, uint64_t n, uint32_t* mask) {
   mask[w] = bits;
 }
 
+__global__ void k_to_f32(float* dst, const double* __restrict__ src, uint64_t n) {
+  const uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  if (i < n) dst[i] = float(src[i]);
+}
+
 // coarse coefficient = mean of the 2^dim children
 __global__ void k_coarsen_k(int dim, uint32_t Nc, const double* __restrict__ kf, double* kc) {
   uint64_t nec = uint64_t(Nc) * Nc * (dim == 3 ? Nc : 1);
@@ -537,6 +542,16 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
   m->structured = true;
   m->dim = d->dim; m->degree = d->degree; m->level = d->level; m->level_min = d->level_min;
   build_kref(m->dim, m->degree, m->kref_h, m->nloc);
+  if (m->degree == 1) {
+    // the cube's reflections give K_ref[a][b] = K_ref[0][a ^ b]; check it before relying on it
+    double mx = 0.0, dev = 0.0;
+    for (int a = 0; a < m->nloc; ++a)
+      for (int b = 0; b < m->nloc; ++b) {
+        mx = std::max(mx, std::fabs(m->kref_h[a * m->nloc + b]));
+        dev = std::max(dev, std::fabs(m->kref_h[a * m->nloc + b] - m->kref_h[a ^ b]));
+      }
+    m->mf_ok = dev <= 1e-14 * mx;
+  }
   const int nl = d->level - d->level_min + 1;
   m->L.resize(nl);
   do {
@@ -568,6 +583,24 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
     for (int i = 0; i < nl && st == FB_OK; ++i) {
       const int lvl = d->level - i;
       st = build_level(m, m->L[i], geom_of(m, lvl), elem_scale(m->dim, lvl));
+    }
+    if (st != FB_OK) break;
+    // matrix-free operator data of the Q1 levels
+    for (int i = 0; i < nl && st == FB_OK && m->mf_ok && m->L[i].St.S; ++i) {
+      Level& L = m->L[i];
+      const double sc = elem_scale(m->dim, d->level - i);
+      L.mf = true;
+      L.M1 = geom_of(m, d->level - i).M1;
+      for (int r = 0; r < m->nloc; ++r) {
+        L.kr64[r] = sc * m->kref_h[r];
+        L.kr32[r] = float(L.kr64[r]);
+      }
+      if (L.k) {
+        st = dalloc(m, &L.k32, L.ne);
+        if (st != FB_OK) break;
+        k_to_f32<<<grid_for(L.ne, 256), 256, 0, m->stream>>>(L.k32, L.k, L.ne);
+        if (cudaGetLastError() != cudaSuccess) st = FB_ERR_CUDA;
+      }
     }
     if (st != FB_OK) break;
     // transfers

@@ -45,6 +45,12 @@ bool debug_enabled() {
   return on == 1;
 }
 
+bool check_enabled() {
+  static int on = -1;
+  if (on < 0) { const char* e = std::getenv("FB_CHECK"); on = ((e && e[0] == '1') || debug_enabled()) ? 1 : 0; }
+  return on == 1;
+}
+
 cudaError_t debug_sync(cudaStream_t s, const char* file, int line) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return cudaSuccess;

@@ -17,6 +17,9 @@ constexpr int kRedThreads = 256;
 // FB_DEBUG=1 in the environment: synchronise after every launch of the multigrid driver
 // and report the source line of a failing launch (debugging aid; never on by default)
 bool debug_enabled();
+// FB_CHECK=1 (implied by FB_DEBUG=1): kernels with self-checks record out-of-range indices
+// instead of using them; the record is reported when the solve ends
+bool check_enabled();
 cudaError_t debug_sync(cudaStream_t s, const char* file, int line);
 void debug_report(cudaError_t e, const char* what, const char* file, int line);
 

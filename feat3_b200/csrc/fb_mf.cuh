@@ -1,0 +1,363 @@
+// Line-tiled matrix-free Q1 operator for structured 3D levels, staged through shared memory
+// by bulk asynchronous copies (cp.async.bulk + mbarrier), with the epilogue of k_mf_q1.
+//
+// A tile is Lt consecutive interior lattice lines (Y0..Y0+Lt-1, fixed Z) minus their two end
+// points, i.e. only rows whose 26 neighbours and 8 cells all exist. Its inputs are contiguous
+// ranges: three x ranges (planes Z-1, Z, Z+1; lines Y0-1..Y0+Lt), two k ranges (cell planes
+// Z-1, Z; cell lines Y0-1..Y0+Lt-1) and one range per streamed epilogue vector (the tile's
+// own lines). One producer warp copies those ranges into an NST-deep ring of stage buffers
+// (each range widened to 16-byte boundaries, which the padded allocations of the driver
+// allow); eight consumer warps compute one row per thread from shared memory. Rows outside
+// the tiles (the lattice boundary planes and lines and the two ends of interior lines) are
+// formed afterwards by the same warps with direct loads.
+//
+// Every wait on an mbarrier is bounded (about one second of %globaltimer); on expiry the
+// kernel records the event in `kerr`, stops taking tiles, waits (bounded) for its copies in
+// flight and returns, so the host can report the failure with the context intact.
+#pragma once
+#include "fb_sell.cuh"
+
+namespace fb {
+
+// ------------------------------------------------------------------ staged epilogues
+// Epilogues whose row-streamed inputs the tiled kernel stages in shared memory. `apply`
+// receives the product s, the row's own x value xc and the staged stream values st[].
+template<typename Epi> struct Staged { static constexpr bool kOk = false; static constexpr int kStreams = 0; };
+
+template<typename T, bool RED>
+struct Staged<EpiJacobi<T, RED>> {
+  using E = EpiJacobi<T, RED>;
+  static constexpr bool kOk = true;
+  static constexpr int kStreams = 2;
+  static const void* stream(const E& e, int i) { return i == 0 ? (const void*)e.rhs : (const void*)e.invd; }
+  static bool input_is_x(const E& e, const void* x) { return e.x == x; }
+  __device__ static bool skip(const E& e) { return smoother_skip<T>(e.skip_src); }
+  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st) {
+    if (skp) {
+      e.out[row] = e.s0 ? e.s0[row] : T(0);
+      return 0.0;
+    }
+    const T d = st[0] - s;
+    if (masked(e.mask, row)) {
+      e.out[row] = xc;
+      return 0.0;
+    }
+    const T t = st[1] * d;
+    e.out[row] = e.omega * t + xc;
+    return RED ? double(d) * double(d) : 0.0;
+  }
+};
+
+template<typename T, bool RED, bool LOW>
+struct Staged<EpiDefect<T, RED, LOW>> {
+  using E = EpiDefect<T, RED, LOW>;
+  static constexpr bool kOk = true;
+  static constexpr int kStreams = 1;
+  static const void* stream(const E& e, int) { return e.rhs; }
+  static bool input_is_x(const E&, const void*) { return true; }
+  __device__ static bool skip(const E&) { return false; }
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T, const T* st) {
+    T d = st[0] - s;
+    if (masked(e.mask, row)) d = T(0);
+    e.def[row] = d;
+    if (LOW) e.def32[row] = float(d);
+    return RED ? double(d) * double(d) : 0.0;
+  }
+};
+
+template<typename T>
+struct Staged<EpiPcgQ<T>> {
+  using E = EpiPcgQ<T>;
+  static constexpr bool kOk = true;
+  static constexpr int kStreams = 0;
+  static const void* stream(const E&, int) { return nullptr; }
+  static bool input_is_x(const E& e, const void* x) { return e.p == x; }  // q . p with p the product's input
+  __device__ static bool skip(const E&) { return false; }
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T xc, const T*) {
+    const T v = masked(e.mask, row) ? T(0) : s;
+    e.q[row] = v;
+    return double(v) * double(xc);
+  }
+};
+
+// ------------------------------------------------------------------ tile geometry
+struct MfTile {
+  uint32_t M1, N;        // lattice points and cells per side
+  uint32_t Lt, tpp;      // lines per tile, tiles per interior plane
+  uint32_t ntiles;       // (M1 - 2) * tpp
+  uint32_t cap_x, cap_k, cap_s;  // bytes reserved per x / k / stream range in a stage
+  uint32_t stage_bytes;
+  uint32_t nbl_items;    // direct-path items: boundary-line chunks
+  uint32_t nedge_items;  // direct-path items: 16 interior lines' end points each
+};
+
+struct TileGeo {
+  uint32_t Z, Y0, lt;
+};
+__device__ __forceinline__ TileGeo tile_geo(const MfTile& G, uint32_t t) {
+  TileGeo g;
+  g.Z = 1 + t / G.tpp;
+  g.Y0 = 1 + (t % G.tpp) * G.Lt;
+  const uint32_t rem = G.M1 - 1 - g.Y0;  // interior lines left in the plane
+  g.lt = rem < G.Lt ? rem : G.Lt;
+  return g;
+}
+
+// ------------------------------------------------------------------ mbarrier / bulk copy
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// wait for the phase of parity `ph` to complete; false after ~1 s
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t ph) {
+  const uint32_t a = smem_u32(b);
+  uint32_t done = 0;
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(ph)
+        : "memory");
+    if (done) return true;
+    if (it == 0) t0 = global_ns();
+    else if ((it & 63) == 0 && global_ns() - t0 > 1000000000ull) return false;
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// range [lo, hi] (elements) of `base` widened to 16-byte boundaries: start element, bytes
+template<typename T>
+__device__ __forceinline__ void widen(uint64_t lo, uint64_t hi, uint64_t& alo, uint32_t& bytes) {
+  constexpr uint64_t E = 16 / sizeof(T);
+  alo = lo & ~(E - 1);
+  bytes = uint32_t(((hi + 1 - alo) * sizeof(T) + 15) & ~uint64_t(15));
+}
+
+// ------------------------------------------------------------------ direct-path row
+// A(k) x for one row with clamped gathers (any row of the level)
+template<typename T>
+__device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __restrict__ x, int32_t row) {
+  const int32_t last = int32_t(A.rows) - 1;
+  const int32_t M1 = int32_t(A.M1), N = M1 - 1;
+  T xv[27];
+#pragma unroll
+  for (int j = 0; j < 27; ++j) {
+    int32_t col = row + A.off[j];
+    col = col < 0 ? 0 : (col > last ? last : col);
+    xv[j] = __ldg(x + col);
+  }
+  const int32_t X = row % M1, t = row / M1, Y = t % M1, Z = t / M1;
+  T s = T(0);
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
+    const int a = (1 - ox) | ((1 - oy) << 1) | ((1 - oz) << 2);
+    const int32_t ex = X - 1 + ox, ey = Y - 1 + oy, ez = Z - 1 + oz;
+    const bool valid = uint32_t(ex) < uint32_t(N) && uint32_t(ey) < uint32_t(N) && uint32_t(ez) < uint32_t(N);
+    const int64_t eidx = valid ? int64_t(ex) + int64_t(N) * (ey + int64_t(N) * ez) : 0;
+    T ke = A.k ? __ldg(A.k + eidx) : T(1);
+    ke = valid ? ke : T(0);
+    T in = T(0);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int dx = ox - 1 + (b & 1), dy = oy - 1 + ((b >> 1) & 1), dz = oz - 1 + ((b >> 2) & 1);
+      in += A.kr[a ^ b] * xv[(dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)];
+    }
+    s += ke * in;
+  }
+  return s;
+}
+
+// ------------------------------------------------------------------ the tiled kernel
+// 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
+template<typename T, typename Epi, int NST, int MINB>
+__global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTile G, const T* __restrict__ x, Epi epi,
+                                                           const T* st0, const T* st1, double* ws, unsigned* counter,
+                                                           double* red_out, unsigned* kerr) {
+  using SE = Staged<Epi>;
+  constexpr int NS = SE::kStreams;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t full[NST], empty[NST];
+  __shared__ double sh[16];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NST; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 8);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const uint32_t M1 = G.M1, N = G.N;
+  const uint32_t W = M1 - 2;  // interior points per line
+  double acc = 0.0;
+  if (warp == 8) {
+    // ---------------- producer
+    if (lane == 0) {
+      uint32_t it = 0;
+      for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it) {
+        const int s = int(it % NST);
+        const uint32_t ph = (it / NST) & 1u;
+        if (it >= NST && !mbar_wait(&empty[s], ph ^ 1u)) {
+          atomicExch(kerr, 1u);
+          break;
+        }
+        const TileGeo g = tile_geo(G, t);
+        unsigned char* st = smem + size_t(s) * G.stage_bytes;
+        uint64_t lo[6];
+        uint32_t by[6];
+        uint32_t total = 0;
+        for (int q = 0; q < 3; ++q) {
+          const uint64_t zp = g.Z - 1 + q;
+          widen<T>((zp * M1 + g.Y0 - 1) * M1, (zp * M1 + g.Y0 + g.lt) * M1 + M1 - 1, lo[q], by[q]);
+          total += by[q];
+        }
+        for (int q = 0; q < 2 && A.k; ++q) {
+          const uint64_t ez = g.Z - 1 + q;
+          widen<T>((ez * N + g.Y0 - 1) * N, (ez * N + g.Y0 + g.lt - 1) * N + N - 1, lo[3 + q], by[3 + q]);
+          total += by[3 + q];
+        }
+        if (NS > 0) {
+          widen<T>((uint64_t(g.Z) * M1 + g.Y0) * M1, (uint64_t(g.Z) * M1 + g.Y0 + g.lt - 1) * M1 + M1 - 1, lo[5], by[5]);
+          total += NS * by[5];
+        }
+        mbar_arrive_tx(&full[s], total);
+        for (int q = 0; q < 3; ++q) bulk_g2s(st + q * G.cap_x, x + lo[q], by[q], &full[s]);
+        for (int q = 0; q < 2 && A.k; ++q) bulk_g2s(st + 3 * G.cap_x + q * G.cap_k, A.k + lo[3 + q], by[3 + q], &full[s]);
+        if (NS > 0) bulk_g2s(st + 3 * G.cap_x + 2 * G.cap_k, st0 + lo[5], by[5], &full[s]);
+        if (NS > 1) bulk_g2s(st + 3 * G.cap_x + 2 * G.cap_k + G.cap_s, st1 + lo[5], by[5], &full[s]);
+      }
+      // copies still in flight (none unless the consumers stopped early)
+      const uint32_t issued = it;
+      for (uint32_t j = issued > NST ? issued - NST : 0; j < issued; ++j)
+        if (!mbar_wait(&full[j % NST], (j / NST) & 1u)) atomicExch(kerr, 2u);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- consumers: one row per thread and tile
+    const bool skp = SE::skip(epi);
+    const uint32_t tid = threadIdx.x;
+    uint32_t it = 0;
+    bool ok = true;
+    for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it) {
+      const int s = int(it % NST);
+      const uint32_t ph = (it / NST) & 1u;
+      if (!mbar_wait(&full[s], ph)) {
+        atomicExch(kerr, 3u);
+        ok = false;
+        break;
+      }
+      const TileGeo g = tile_geo(G, t);
+      const unsigned char* st = smem + size_t(s) * G.stage_bytes;
+      if (tid < g.lt * W) {
+        const uint32_t ly = tid / W, X = 1 + tid % W;
+        constexpr uint64_t E = 16 / sizeof(T);
+        const T* xs[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          const uint64_t zp = g.Z - 1 + q;
+          const uint64_t l0 = (zp * M1 + g.Y0 - 1) * M1;
+          xs[q] = reinterpret_cast<const T*>(st + q * G.cap_x) + (l0 & (E - 1)) + (ly + 1) * M1 + X;
+        }
+        T xv[27];
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+          for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) xv[dz * 9 + dy * 3 + dx] = xs[dz][(int(dy) - 1) * int(M1) + dx - 1];
+        T kv[8];
+        if (A.k) {
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const uint64_t ez = g.Z - 1 + q;
+            const uint64_t c0 = (ez * N + g.Y0 - 1) * N;
+            const T* ks = reinterpret_cast<const T*>(st + 3 * G.cap_x + q * G.cap_k) + (c0 & (E - 1)) + ly * N + (X - 1);
+            kv[q * 4 + 0] = ks[0];
+            kv[q * 4 + 1] = ks[1];
+            kv[q * 4 + 2] = ks[N];
+            kv[q * 4 + 3] = ks[N + 1];
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < 8; ++e) kv[e] = T(1);
+        }
+        T s = T(0);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
+          const int a = (1 - ox) | ((1 - oy) << 1) | ((1 - oz) << 2);
+          T in = T(0);
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            const int dx = ox + (b & 1), dy = oy + ((b >> 1) & 1), dz = oz + ((b >> 2) & 1);
+            in += A.kr[a ^ b] * xv[dz * 9 + dy * 3 + dx];
+          }
+          s += kv[oz * 4 + oy * 2 + ox] * in;
+        }
+        const uint32_t row = (g.Z * M1 + g.Y0 + ly) * M1 + X;
+        T sv[NS > 0 ? NS : 1];
+        if (NS > 0) {
+          const uint64_t r0 = (uint64_t(g.Z) * M1 + g.Y0) * M1;
+          const T* ss = reinterpret_cast<const T*>(st + 3 * G.cap_x + 2 * G.cap_k) + (r0 & (E - 1)) + ly * M1 + X;
+          sv[0] = ss[0];
+          if (NS > 1) sv[NS > 1 ? 1 : 0] = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[0];
+        }
+        acc += SE::apply(epi, skp, row, s, xv[13], sv);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    // ---------------- direct path: boundary lines and the end points of interior lines
+    if (ok) {
+      const uint32_t cpl = (M1 + 31) / 32;  // chunks per boundary line
+      const uint32_t nitems = G.nbl_items + G.nedge_items;
+      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
+        int32_t row = -1;
+        if (item < G.nbl_items) {
+          const uint32_t bl = item / cpl, X = (item % cpl) * 32 + lane;
+          uint32_t Y, Z;
+          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl % M1; }
+          else { const uint32_t r = bl - 2 * M1; Z = 1 + r / 2; Y = (r & 1) ? M1 - 1 : 0; }
+          if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
+        } else {
+          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
+          if (li < W * W) {
+            const uint32_t Y = 1 + li % W, Z = 1 + li / W;
+            row = int32_t((Z * M1 + Y) * M1 + ((lane & 1) ? M1 - 1 : 0));
+          }
+        }
+        if (row >= 0) {
+          const T s = mf_row_direct<T>(A, x, row);
+          acc += epi(uint32_t(row), s);
+        }
+      }
+    }
+  }
+  if (Epi::kReduce) {
+    const double blk = block_sum<288>(acc, sh);
+    reduce_finish<288>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+}  // namespace fb

@@ -16,6 +16,7 @@
 //   * the smoother's initial-norm test (skip on a non-finite or <= eps^2 defect) is kept:
 //     the norm is reduced inside the kernel that produces the defect and read by the next.
 #include "fb_mg_internal.cuh"
+#include "fb_mf.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -229,13 +230,23 @@ __global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __res
 
 // PCG update: alpha = gamma / qp; x += alpha p; r -= alpha q; ||r||^2 (+ FP32 copy of r)
 // (pcg.hpp:241-251 with the |alpha| < eps shortcut of dense_vector.hpp:891-895)
+// When s1 != nullptr the kernel also forms the first pre-smoothing step of the next V-cycle
+// from zero, s1 = omega * filter_cor(invd o r) in the V-cycle's type (k_jacobi0 on the new r;
+// the smoother's skip test is not needed there: the next V-cycle runs only after the host
+// has found ||r|| finite and above the tolerance, and a skipped smoother with nu >= 2 is
+// restored by the second step, which sees the same skip test).
 template<bool LOW>
 __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float* r32, const double* __restrict__ p,
                                                     const double* __restrict__ q, const DevScalars* sc, uint32_t n,
-                                                    double* ws, unsigned* counter, double* rr_out) {
+                                                    double* ws, unsigned* counter, double* rr_out,
+                                                    void* s1, const void* invd, const uint32_t* mask, double omega) {
+  using T = typename std::conditional<LOW, float, double>::type;
   __shared__ double sh[8];
   const double alpha = sc->gamma / sc->qp;
   const bool upd = fabs(alpha) >= eps_of<double>();
+  T* s1t = static_cast<T*>(s1);
+  const T* invt = static_cast<const T*>(invd);
+  const T om = T(omega);
   double acc = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double ri = r[i];
@@ -245,6 +256,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
       r[i] = ri;
     }
     if (LOW) r32[i] = float(ri);
+    if (s1t) s1t[i] = masked(mask, i) ? T(0) : om * (invt[i] * T(ri));
     acc += ri * ri;
   }
   const double blk = block_sum<256>(acc, sh);
@@ -339,12 +351,108 @@ template<> struct Prec<float> {
 
 // dispatch a SELL launch on the value storage of the configured precision
 static bool use_stencil(const fb_mg* m, const Level& L) {
-  return m->cfg.format == FB_FORMAT_STENCIL && L.St.S > 0;
+  return m->cfg.format != FB_FORMAT_SELL && L.St.S > 0;
+}
+static bool use_matfree(const fb_mg* m, const Level& L) {
+  return m->cfg.format == FB_FORMAT_MATFREE && L.mf;
+}
+// the structured formats replace the CSR transfer matrices by the matrix-free Q1 transfers
+static bool use_q1_transfer(const fb_mg* m, const Level& L) {
+  return m->cfg.format != FB_FORMAT_SELL && L.q1_transfer;
+}
+
+// self-check record of the matrix-free kernels (FB_CHECK=1): report and clear it
+static int check_self_checks(fb_mg* m) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(m->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return FB_OK;
+  unsigned long long h = 0;
+  FB_CUDA(cudaMemcpyAsync(&h, m->dbg_err, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  if (!h) return FB_OK;
+  FB_CUDA(cudaMemsetAsync(m->dbg_err, 0, sizeof(h), m->stream));
+  const unsigned kind = unsigned(h >> 62);
+  std::fprintf(stderr, "feat3_b200: k_mf_q1 self-check: %s (row %llu, slot %llu)\n",
+               kind == 1 ? "x index out of range" : (kind == 2 ? "cell index out of range" : "geometry mismatch"),
+               (h >> 8) & 0xffffffffull, h & 0xffull);
+  return FB_ERR_CUDA;
+}
+
+// line-tiled staged launch (3D levels with at least 16 interior points per line)
+template<typename T, typename Epi>
+static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
+                           double* red_out) {
+  using SE = Staged<Epi>;
+  constexpr int NS = SE::kStreams;
+  constexpr int NST = sizeof(T) == 4 ? 4 : 3;
+  constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
+  const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
+  auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
+  MfTile G;
+  G.M1 = M1; G.N = N;
+  G.Lt = std::max<uint32_t>(1, 256 / W);
+  G.tpp = (W + G.Lt - 1) / G.Lt;
+  G.ntiles = W * G.tpp;
+  G.cap_x = r16(uint64_t(G.Lt + 2) * M1 * sizeof(T)) + 32;
+  G.cap_k = v.k ? r16(uint64_t(G.Lt + 1) * N * sizeof(T)) + 32 : 0;
+  G.cap_s = NS ? r16(uint64_t(G.Lt) * M1 * sizeof(T)) + 32 : 0;
+  G.stage_bytes = (3 * G.cap_x + 2 * G.cap_k + NS * G.cap_s + 127) & ~127u;
+  G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
+  G.nedge_items = (W * W + 15) / 16;
+  const size_t dyn = size_t(NST) * G.stage_bytes;
+  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB>;
+  static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
+  if (dyn > attr) {
+    FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+    attr = dyn;
+  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, 288, dyn) != cudaSuccess || bps < 1) {
+    cudaGetLastError();
+    bps = 1;
+  }
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(G.ntiles, uint32_t(bps) * kSMs));
+  const T* s0 = NS > 0 ? static_cast<const T*>(SE::stream(epi, 0)) : nullptr;
+  const T* s1 = NS > 1 ? static_cast<const T*>(SE::stream(epi, 1)) : nullptr;
+  fn<<<grid, 288, dyn, m->stream>>>(v, G, x, epi, s0, s1, m->ws, m->counter, red_out, m->kerr);
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
+template<typename T, typename Epi, int DIM>
+static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* red_out) {
+  MfView<T, DIM> v;
+  v.rows = L.n; v.nchunks = (L.n + 31) / 32; v.M1 = L.M1; v.ne = L.ne;
+  v.err = check_enabled() ? m->dbg_err : nullptr;
+  if constexpr (std::is_same<T, double>::value) {
+    v.k = L.k;
+    for (int r = 0; r < (1 << DIM); ++r) v.kr[r] = L.kr64[r];
+  } else {
+    v.k = L.k ? L.k32 : nullptr;
+    for (int r = 0; r < (1 << DIM); ++r) v.kr[r] = L.kr32[r];
+  }
+  for (int j = 0; j < (DIM == 3 ? 27 : 9); ++j) v.off[j] = L.St.off[j];
+  if constexpr (DIM == 3 && Staged<Epi>::kOk) {
+    if (L.M1 >= 18 && Staged<Epi>::input_is_x(epi, x) && !v.err) return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
+  }
+  auto fn = k_mf_q1<T, Epi, DIM>;
+  if (debug_enabled())
+    debug_check_ptrs("k_mf_q1", {(const void*)v.k, (const void*)x, (const void*)m->ws, (const void*)m->counter,
+                                 (const void*)red_out});
+  fn<<<occupancy_grid((const void*)fn, v.nchunks), 256, 0, m->stream>>>(v, x, epi, m->ws, m->counter, red_out);
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  if (v.err && debug_enabled()) FB_TRY(check_self_checks(m));
+  return FB_OK;
 }
 
 // level operator A x with an epilogue, on the storage the configuration selects
 template<typename T, typename Epi>
 static int spmv_L(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* red) {
+  if (use_matfree(m, L)) {
+    if (m->dim == 3) return launch_mf_D<T, Epi, 3>(m, L, x, epi, red);
+    return launch_mf_D<T, Epi, 2>(m, L, x, epi, red);
+  }
   const bool st = use_stencil(m, L);
   if constexpr (std::is_same<T, double>::value) {
     if (st) return launch_stencil<double, double, double, Epi>(m, L, FB_PREC_F64, x, epi, red);
@@ -363,7 +471,17 @@ static int spmv_L(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* 
 template<typename T, typename Epi>
 static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
   const Level& L = m->L[l];
-  if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
+  if (use_q1_transfer(m, L)) {
+    if constexpr (std::is_same<Epi, EpiRestrict<T>>::value) {
+      if (L.tr.dim == 3) {
+        constexpr int ZB = 2;
+        const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, (L.tr.Mc1 + ZB - 1) / ZB);
+        k_rest_q1_3d<T, ZB><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        return FB_OK;
+      }
+    }
     const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, L.tr.dim == 3 ? L.tr.Mc1 : 1);
     k_rest_q1<T, Epi><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
     m->launches++;
@@ -378,7 +496,17 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
 template<typename T, typename Epi>
 static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
   const Level& L = m->L[l];
-  if (m->cfg.format == FB_FORMAT_STENCIL && L.q1_transfer) {
+  if (use_q1_transfer(m, L)) {
+    if constexpr (std::is_same<Epi, EpiProlong<T>>::value) {
+      if (L.tr.dim == 3) {
+        constexpr int ZB = 8;
+        const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + ZB - 1) / ZB);
+        k_prol_q1_3d<T, ZB><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        return FB_OK;
+      }
+    }
     const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, L.tr.dim == 3 ? L.tr.Mf1 : 1);
     k_prol_q1<T, Epi><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xc, epi);
     m->launches++;
@@ -423,7 +551,7 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     Level& C = m->L[l + 1];
     const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
     const double* bn = (l == 0) ? rhs_top_sumsq : &m->sc->lvl[2 * l];
-    const bool need_s1 = (l == 0) || nu < 2;
+    const bool need_s1 = (l == 0) ? !m->top_s1 : nu < 2;
     FB_TRY(presmooth<T>(m, l, b, bn, need_s1, &sol[l]));
     EpiDefect<T, false, false> ed{Prec<T>::def(L), b, L.mask, nullptr};
     FB_TRY(spmv_L<T>(m, L, sol[l], ed, nullptr));
@@ -528,6 +656,12 @@ struct Stop {
 };
 
 // ------------------------------------------------------------------ solver bodies
+// PCG outer with nu >= 2 on two or more levels: the PCG update kernel also forms the first
+// pre-smoothing step of the next V-cycle on the finest level (k_jacobi0 is not launched there)
+static bool fuse_s1(const fb_mg* m) {
+  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1;
+}
+
 // outer defect r = filter_def(b - A x), ||r||^2, FP32 copy for the mixed V-cycle
 static int outer_defect(fb_mg* m) {
   Level& L = m->L[0];
@@ -558,7 +692,10 @@ static int body(fb_mg* m) {
   const uint32_t n = m->L[0].n;
   const bool low = m->cfg.precision != FB_PREC_F64;
   const void* z = nullptr;
-  FB_TRY(precond(m, &z));
+  m->top_s1 = fuse_s1(m);
+  const int pst = precond(m, &z);
+  m->top_s1 = false;
+  FB_TRY(pst);
   if (m->cfg.outer == FB_OUTER_PCG) {
     // gamma' = r . z ; p = z + beta p ; q = A p ; x, r update
     if (low) k_dot_rz<float><<<occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz);
@@ -574,8 +711,14 @@ static int body(fb_mg* m) {
     FB_CHECK_LAUNCH();
     EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
     FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
-    if (low) k_pcg_update<true><<<occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
-    else     k_pcg_update<false><<<occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1), 256, 0, m->stream>>>(m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr);
+    Level& L0 = m->L[0];
+    const bool fs = fuse_s1(m);
+    if (low) k_pcg_update<true><<<occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1), 256, 0, m->stream>>>(
+        m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x32 : nullptr,
+        L0.invd32, L0.mask, m->cfg.omega_rich);
+    else     k_pcg_update<false><<<occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1), 256, 0, m->stream>>>(
+        m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x64 : nullptr,
+        L0.invd64, L0.mask, m->cfg.omega_rich);
     m->launches++;
     FB_CHECK_LAUNCH();
   } else {
@@ -638,13 +781,16 @@ static int ensure_vectors(fb_mg* m, int prec) {
         k_cvt<float, double><<<ew_grid(L.R.nnz), 256, 0, m->stream>>>(L.R.v32, L.R.v64, L.R.nnz);
         FB_CHECK_LAUNCH();
       }
-      if (L.St.S && prec == FB_PREC_F32 && !L.St.v32) {
+      const bool mf = m->cfg.format == FB_FORMAT_MATFREE && L.mf;
+      const bool need_st = m->cfg.format != FB_FORMAT_SELL && L.St.S && !mf;
+      const bool need_sell = !mf && !need_st;
+      if (need_st && prec == FB_PREC_F32 && !L.St.v32) {
         const uint64_t np = uint64_t(L.St.nchunks) * ((L.St.S + 1) / 2) * 32 * 2;
         FB_TRY(dalloc(m, &L.St.v32, np));
         k_stencil_pack<float><<<ew_grid(np), 256, 0, m->stream>>>(L.St.v32, L.St.v64, L.St.nchunks, L.St.S, 1.0);
         FB_CHECK_LAUNCH();
       }
-      if (L.St.S && prec == FB_PREC_F16 && !L.St.v16) {
+      if (need_st && prec == FB_PREC_F16 && !L.St.v16) {
         const uint64_t ns = uint64_t(L.St.nchunks) * L.St.S * 32;
         unsigned long long* dmax = nullptr;
         FB_TRY(dalloc(m, &dmax, 1));
@@ -663,12 +809,12 @@ static int ensure_vectors(fb_mg* m, int prec) {
                                                                      1.0 / double(L.St.scale16));
         FB_CHECK_LAUNCH();
       }
-      if (prec == FB_PREC_F32 && !L.A.v32) {
+      if (need_sell && prec == FB_PREC_F32 && !L.A.v32) {
         FB_TRY(dalloc(m, &L.A.v32, L.A.nent));
         k_cvt<float, double><<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v32, L.A.v64, L.A.nent);
         FB_CHECK_LAUNCH();
       }
-      if (prec == FB_PREC_F16 && !L.A.v16) {
+      if (need_sell && prec == FB_PREC_F16 && !L.A.v16) {
         // per-level scale: the largest magnitude maps to 2^14 (headroom below 65504)
         unsigned long long* dmax = nullptr;
         FB_TRY(dalloc(m, &dmax, 1));
@@ -841,6 +987,10 @@ int common_init(fb_mg* m) {
   FB_TRY(dalloc(m, &m->ws, 8192));
   FB_TRY(dalloc(m, &m->counter, 4));
   FB_CUDA(cudaMemsetAsync(m->counter, 0, 4 * sizeof(unsigned), m->stream));
+  FB_TRY(dalloc(m, &m->dbg_err, 1));
+  FB_CUDA(cudaMemsetAsync(m->dbg_err, 0, sizeof(unsigned long long), m->stream));
+  FB_TRY(dalloc(m, &m->kerr, 1));
+  FB_CUDA(cudaMemsetAsync(m->kerr, 0, sizeof(unsigned), m->stream));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
   FB_CUDA(cudaEventCreate(&m->ev0));
@@ -879,6 +1029,17 @@ int finish_levels(fb_mg* m) {
   return FB_OK;
 }
 
+// a bounded wait inside a staged kernel expired: report it (and clear the flag)
+static int check_kernel_waits(fb_mg* m) {
+  unsigned h = 0;
+  FB_CUDA(cudaMemcpyAsync(&h, m->kerr, sizeof(h), cudaMemcpyDeviceToHost, m->stream));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  if (!h) return FB_OK;
+  FB_CUDA(cudaMemsetAsync(m->kerr, 0, sizeof(unsigned), m->stream));
+  if (debug_enabled()) std::fprintf(stderr, "feat3_b200: staged kernel wait expired (code %u)\n", h);
+  return FB_ERR_TIMEOUT;
+}
+
 // ------------------------------------------------------------------ solve
 int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info) {
   if (!m->configured) return FB_ERR_NOT_READY;
@@ -896,6 +1057,17 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
     k_fill<double><<<ew_grid(n), 256, 0, s>>>(m->p, 0.0, n);
     m->launches += 2;
     FB_CHECK_LAUNCH();
+    if (fuse_s1(m)) {
+      // first pre-smoothing step of the first V-cycle (later ones come from k_pcg_update)
+      Level& L0 = m->L[0];
+      const double om = m->cfg.omega_rich;
+      if (m->cfg.precision == FB_PREC_F64)
+        k_jacobi0<double><<<ew_grid(n), 256, 0, s>>>(L0.x64, m->r, L0.invd64, L0.mask, &m->sc->rr, om, n);
+      else
+        k_jacobi0<float><<<ew_grid(n), 256, 0, s>>>(L0.x32, m->r32, L0.invd32, L0.mask, &m->sc->rr, float(om), n);
+      m->launches++;
+      FB_CHECK_LAUNCH();
+    }
   }
   FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, sizeof(double), cudaMemcpyDeviceToHost, s));
   FB_CUDA(cudaStreamSynchronize(s));
@@ -915,6 +1087,8 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
   FB_CUDA(cudaMemcpyAsync(sol, m->xb, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   FB_CUDA(cudaEventRecord(m->ev1, s));
   FB_CUDA(cudaEventSynchronize(m->ev1));
+  FB_TRY(check_kernel_waits(m));
+  if (check_enabled()) FB_TRY(check_self_checks(m));
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, m->ev0, m->ev1);
   if (info) {
@@ -950,7 +1124,7 @@ int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (!m || !c) return FB_ERR_INVALID;
   if (c->nu < 1 || c->nu > 64 || c->max_iter < 0 || !(c->tol_rel >= 0.0) ||
       c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3 ||
-      c->format < 0 || c->format > 1)
+      c->format < 0 || c->format > 2)
     return FB_ERR_INVALID;
   if (c->coarse == FB_COARSE_PCG && !m->coarse_csr.rp) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;
@@ -1084,8 +1258,11 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
   FB_CUDA(cudaSetDevice(m->device));
   Level& L = m->L[level];
   const bool low = prec != FB_PREC_F64;
-  if ((low && !L.x32) || (!low && !L.x64) || (prec == FB_PREC_F16 && !L.A.v16) || (prec == FB_PREC_F32 && !L.A.v32))
-    return FB_ERR_NOT_READY;
+  bool stored;
+  if (use_matfree(m, L)) stored = true;
+  else if (use_stencil(m, L)) stored = prec == FB_PREC_F64 ? L.St.v64 != nullptr : (prec == FB_PREC_F32 ? L.St.v32 != nullptr : L.St.v16 != nullptr);
+  else stored = prec == FB_PREC_F64 ? L.A.v64 != nullptr : (prec == FB_PREC_F32 ? L.A.v32 != nullptr : L.A.v16 != nullptr);
+  if ((low && !L.x32) || (!low && !L.x64) || !stored) return FB_ERR_NOT_READY;
   if (which == 2 && (level != 0 || low)) return FB_ERR_INVALID;
   const int saved = m->cfg.precision;
   m->cfg.precision = prec;
@@ -1108,6 +1285,7 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
   for (int i = 0; i < reps && st == FB_OK; ++i) st = one();
   if (st == FB_OK) st = cuda_status(cudaEventRecord(m->ev1, m->stream));
   if (st == FB_OK) st = cuda_status(cudaEventSynchronize(m->ev1));
+  if (st == FB_OK) st = check_kernel_waits(m);
   m->cfg.precision = saved;
   if (st != FB_OK) return st;
   float t = 0.0f;

@@ -77,6 +77,12 @@ struct Level {
   int N = 0;             // cells per side
   uint64_t ne = 0;       // elements
   double* k = nullptr;   // per-element coefficient (device)
+  // matrix-free Q1 operator (structured Q1 levels)
+  bool mf = false;
+  uint32_t M1 = 0;       // lattice points per side
+  double kr64[8] = {0};  // (h/2)^(dim-2) K_ref[0][r]
+  float kr32[8] = {0};
+  float* k32 = nullptr;  // FP32 copy of k
 };
 
 }  // namespace fb
@@ -94,6 +100,7 @@ struct fb_mg {
   int dim = 0, degree = 0, level = 0, level_min = 0;
   int nloc = 0;
   double* kref = nullptr;        // unit-coefficient element matrix on [-1,1]^d (device)
+  bool mf_ok = false;            // K_ref[a][b] == K_ref[0][a^b] (Q1 cube symmetry): matrix-free apply possible
   std::vector<double> kref_h;
   // coarse level as CSR (for the single-CTA CG coarse solver) and its work vectors
   fb::DevCsr coarse_csr;
@@ -117,6 +124,9 @@ struct fb_mg {
   int g_body_key = -1;
   int launches = 0;
   int body_launches = 0;
+  bool top_s1 = false;
+  unsigned long long* dbg_err = nullptr;  // FB_DEBUG=1: device word for kernel self-checks
+  unsigned* kerr = nullptr;               // set by a staged kernel whose bounded wait expired                   // finest-level first smoothing step already formed (fused)
   double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
   double* adj = nullptr;                 // adjoint right-hand side
 };
@@ -132,7 +142,8 @@ template<typename T>
 int dalloc(fb_mg* m, T** p, uint64_t n) {
   *p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMalloc((void**)p, sizeof(T) * n) != cudaSuccess) { *p = nullptr; cudaGetLastError(); return FB_ERR_ALLOC; }
+  // 64 bytes of slack: staged kernels widen their copies to 16-byte boundaries
+  if (cudaMalloc((void**)p, sizeof(T) * n + 64) != cudaSuccess) { *p = nullptr; cudaGetLastError(); return FB_ERR_ALLOC; }
   m->allocs.push_back(*p);
   return FB_OK;
 }

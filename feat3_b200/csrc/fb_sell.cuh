@@ -317,28 +317,6 @@ template<> struct Pack8<float> {
   }
 };
 
-// x gathers: the offsets come in runs of three (dx = -1, 0, +1) around each (dy, dz) line
-// centre, so on interior chunks each run is one coalesced load of x[b + lane] plus one
-// two-lane load of the halo (x[b-1] for lane 0, x[b+32] for lane 31) and two shuffles,
-// instead of three 128-byte loads: a third of the L2->SM traffic of the gathers.
-template<int S>
-__device__ __forceinline__ void gather_runs(const float* __restrict__ x, const int32_t* off, int32_t row0, int lane,
-                                            float* xv) {
-#pragma unroll
-  for (int r = 0; r < S / 3; ++r) {
-    const int32_t b = row0 + off[3 * r + 1];  // centre of the run
-    const float c = __ldg(x + b + lane);
-    float e = 0.0f;
-    if (lane == 0) e = __ldg(x + b - 1);
-    else if (lane == 31) e = __ldg(x + b + 32);
-    const float lft = __shfl_up_sync(0xffffffffu, c, 1);
-    const float rgt = __shfl_down_sync(0xffffffffu, c, 1);
-    xv[3 * r + 0] = lane == 0 ? e : lft;
-    xv[3 * r + 1] = c;
-    xv[3 * r + 2] = lane == 31 ? e : rgt;
-  }
-}
-
 template<typename VT, typename Epi, int S>
 __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, const float* __restrict__ x, Epi epi,
                                                            double* ws, unsigned* counter, double* red_out) {
@@ -355,17 +333,6 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
     const int32_t row = row0 + lane;
     const VT* vp = val + (size_t(c) * G * 32 + lane) * W;
     const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
-    float xv[S];
-    if (inside) {
-      gather_runs<S>(x, A.off, row0, lane, xv);
-    } else {
-#pragma unroll
-      for (int j = 0; j < S; ++j) {
-        int32_t col = row + A.off[j];
-        col = col < 0 ? 0 : (col > last ? last : col);
-        xv[j] = __ldg(x + col);
-      }
-    }
     float sum = 0.0f;
 #pragma unroll
     for (int g = 0; g < G; ++g) {
@@ -374,13 +341,110 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
 #pragma unroll
       for (int e = 0; e < W; ++e) {
         const int j = g * W + e;
-        if (j < S) sum += v[e] * xv[j];
+        if (j < S) {
+          int32_t col = row + A.off[j];
+          if (!inside) col = col < 0 ? 0 : (col > last ? last : col);
+          sum += v[e] * __ldg(x + col);
+        }
       }
     }
     if (row <= last) {
       if (sizeof(VT) == 2) sum *= A.scale;
       acc += epi(uint32_t(row), sum);
     }
+  }
+  if (Epi::kReduce) {
+    const double blk = block_sum<256>(acc, sh);
+    reduce_finish<256>(blk, ws, counter, red_out, sh, false);
+  }
+}
+
+// ------------------------------------------------------------------ matrix-free Q1 operator
+// y = A(k) x for a structured Q1 level without reading a matrix: A(k) = sum_e k_e K_e with
+// K_e = (h/2)^(dim-2) K_ref, K_ref the unit-coefficient element matrix of [-1,1]^dim. Local
+// vertex a of a cell has bit d set when it lies at the upper end of the cell in direction d.
+// On the cube, K_ref[a][b] depends only on a xor b (a reflection of the cube maps vertex a
+// to vertex 0 and keeps the Laplacian), so kr[r] = (h/2)^(dim-2) K_ref[0][r] carries the
+// whole element matrix. Row i sums over the (up to 2^dim) cells around lattice point i;
+// cells outside the domain are skipped, so boundary rows equal the assembled matrix rows.
+template<typename T, int DIM>
+struct MfView {
+  uint32_t rows, nchunks;
+  uint32_t M1;          // lattice points per side (= cells per side + 1)
+  const T* k;           // per-cell coefficient, lexicographic (nullptr = 1)
+  uint64_t ne;          // number of cells
+  unsigned long long* err;  // debugging aid: first out-of-range index is recorded here (nullptr = off)
+  T kr[1 << DIM];
+  int32_t off[DIM == 3 ? 27 : 9];  // neighbour offsets, slot j = (dz+1)*9 + (dy+1)*3 + (dx+1)
+};
+
+template<typename T, typename Epi, int DIM>
+__global__ void __launch_bounds__(256) k_mf_q1(MfView<T, DIM> A, const T* __restrict__ x, Epi epi,
+                                               double* ws, unsigned* counter, double* red_out) {
+  constexpr int S = DIM == 3 ? 27 : 9;
+  constexpr int NE = 1 << DIM;
+  __shared__ double sh[8];
+  const int lane = threadIdx.x & 31;
+  const uint32_t wpb = blockDim.x >> 5;
+  const int32_t last = int32_t(A.rows) - 1;
+  const int32_t M1 = int32_t(A.M1), N = M1 - 1;
+  double acc = 0.0;
+  if (A.err) {
+    const uint64_t m1 = A.M1;
+    const uint64_t want = DIM == 3 ? m1 * m1 * m1 : m1 * m1;
+    const uint64_t nc = DIM == 3 ? uint64_t(N) * N * N : uint64_t(N) * N;
+    if (want != A.rows || (A.k && nc != A.ne) || A.nchunks != (A.rows + 31) / 32) {
+      atomicCAS(A.err, 0ull, 3ull << 62);
+      return;
+    }
+  }
+  for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < A.nchunks; c += gridDim.x * wpb) {
+    const int32_t row0 = int32_t(c) * 32;
+    const int32_t row = row0 + lane;
+    const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
+    T xv[S];
+#pragma unroll
+    for (int j = 0; j < S; ++j) {
+      int32_t col = row + A.off[j];
+      if (!inside) col = col < 0 ? 0 : (col > last ? last : col);
+      if (A.err && uint32_t(col) > uint32_t(last)) {
+        atomicCAS(A.err, 0ull, (1ull << 62) | (uint64_t(uint32_t(row)) << 8) | uint64_t(j));
+        col = 0;
+      }
+      xv[j] = __ldg(x + col);
+    }
+    const int32_t rr = row <= last ? row : last;
+    const int32_t X = rr % M1;
+    const int32_t t = rr / M1;
+    const int32_t Y = DIM == 3 ? t % M1 : t;
+    const int32_t Z = DIM == 3 ? t / M1 : 0;
+    T s = T(0);
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+      // cell (X-1+ox, Y-1+oy, Z-1+oz); the row's vertex in it is a = (1-ox, 1-oy, 1-oz)
+      const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
+      const int a = (1 - ox) | ((1 - oy) << 1) | (DIM == 3 ? (1 - oz) << 2 : 0);
+      const int32_t ex = X - 1 + ox, ey = Y - 1 + oy, ez = DIM == 3 ? Z - 1 + oz : 0;
+      const bool valid = uint32_t(ex) < uint32_t(N) && uint32_t(ey) < uint32_t(N) &&
+                         (DIM == 2 || uint32_t(ez) < uint32_t(N));
+      int64_t eidx = valid ? int64_t(ex) + int64_t(N) * (ey + int64_t(N) * ez) : 0;
+      if (A.err && A.k && uint64_t(eidx) >= A.ne) {
+        atomicCAS(A.err, 0ull, (2ull << 62) | (uint64_t(uint32_t(row)) << 8) | uint64_t(e));
+        eidx = 0;
+      }
+      T ke = A.k ? __ldg(A.k + eidx) : T(1);
+      ke = valid ? ke : T(0);
+      T in = T(0);
+#pragma unroll
+      for (int b = 0; b < NE; ++b) {
+        const int dx = ox - 1 + (b & 1), dy = oy - 1 + ((b >> 1) & 1);
+        const int dz = DIM == 3 ? oz - 1 + ((b >> 2) & 1) : 0;
+        const int j = DIM == 3 ? (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1) : (dy + 1) * 3 + (dx + 1);
+        in += A.kr[a ^ b] * xv[j];
+      }
+      s += ke * in;
+    }
+    if (row <= last) acc += epi(uint32_t(row), s);
   }
   if (Epi::kReduce) {
     const double blk = block_sum<256>(acc, sh);
@@ -498,6 +562,130 @@ __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restri
     const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
   }
+}
+
+// 3D prolongation + coarse-grid correction (EpiProlong: sol += filter_cor(P x_c)) for ZB
+// consecutive fine planes per thread, launched on a (ceil(Mf1/32), ceil(Mf1/8), ceil(Mf1/ZB))
+// grid of 32x8 blocks. The ZB/2+1 coarse planes behind the slab are read once, and all
+// iterate values of the slab are loaded before the first store, so a thread keeps ~30
+// independent loads in flight. Per fine point the terms and their order are those of
+// k_prol_q1 (the CSR row order plus exact zeros).
+template<typename T, int ZB>
+__global__ void __launch_bounds__(256) k_prol_q1_3d(Q1Transfer g, const T* __restrict__ xc, T* __restrict__ sol,
+                                                    const uint32_t* __restrict__ mask) {
+  static_assert(ZB % 2 == 0, "slabs start on even planes");
+  const uint32_t X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z0 = blockIdx.z * ZB;
+  if (X >= g.Mf1 || Y >= g.Mf1) return;
+  const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
+  constexpr int NQ = ZB / 2 + 1;
+  T v[NQ][4];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    uint32_t cz = Z0 / 2 + q;
+    cz = cz < g.Mc1 ? cz : g.Mc1 - 1;  // planes past the lattice feed no fine point
+    const size_t r0 = (size_t(cz) * g.Mc1 + cy0) * g.Mc1, r1 = (size_t(cz) * g.Mc1 + cy1) * g.Mc1;
+    v[q][0] = xc[r0 + cx0]; v[q][1] = xc[r0 + cx1];
+    v[q][2] = xc[r1 + cx0]; v[q][3] = xc[r1 + cx1];
+  }
+  const size_t plane = size_t(g.Mf1) * g.Mf1;
+  const size_t i0 = X + size_t(g.Mf1) * (Y + size_t(g.Mf1) * Z0);
+  T old[ZB];
+  uint32_t mw[ZB];
+#pragma unroll
+  for (int z = 0; z < ZB; ++z) {
+    const bool in = Z0 + z < g.Mf1;
+    const size_t i = in ? i0 + z * plane : i0;
+    old[z] = sol[i];
+    mw[z] = mask ? __ldg(mask + (i >> 5)) : 0u;
+  }
+  const T hx = (X & 1) ? T(0.5) : T(1), hy = (Y & 1) ? T(0.5) : T(1);
+  const T wy1 = (Y & 1) ? T(1) : T(0);
+#pragma unroll
+  for (int z = 0; z < ZB; ++z) {
+    if (Z0 + z >= g.Mf1) break;
+    const size_t i = i0 + z * plane;
+    const T w = hx * hy * ((z & 1) ? T(0.5) : T(1));
+    const T wx1 = (X & 1) ? w : T(0);
+    const T wz1 = (z & 1) ? T(1) : T(0);
+    const int q0 = z >> 1, q1 = (z + 1) >> 1;
+    T s = T(0);
+    s += w * v[q0][0];
+    s += wx1 * v[q0][1];
+    s += (wy1 * w) * v[q0][2];
+    s += (wy1 * wx1) * v[q0][3];
+    s += (wz1 * w) * v[q1][0];
+    s += (wz1 * wx1) * v[q1][1];
+    s += (wz1 * wy1 * w) * v[q1][2];
+    s += (wz1 * wy1 * wx1) * v[q1][3];
+    if (!((mw[z] >> (i & 31)) & 1u)) sol[i] = T(1) * s + old[z];
+  }
+}
+
+// 3D restriction (EpiRestrict: rhs_c = filter_def(R d), ||rhs_c||^2, optional first
+// pre-smoothing step sol1 = omega filter_cor(invd o rhs_c)) for ZB consecutive coarse planes
+// per thread; fine plane 2Zc+1 is shared by coarse planes Zc and Zc+1 and read once.
+// Launched on a (ceil(Mc1/32), ceil(Mc1/8), ceil(Mc1/ZB)) grid of 32x8 blocks. Per coarse
+// point the terms and their order are those of k_rest_q1.
+template<typename T, int ZB>
+__global__ void __launch_bounds__(256) k_rest_q1_3d(Q1Transfer g, const T* __restrict__ xf, EpiRestrict<T> epi,
+                                                    double* ws, unsigned* counter, double* red_out) {
+  __shared__ double sh[8];
+  const int X = int(blockIdx.x * 32 + threadIdx.x), Y = int(blockIdx.y * 8 + threadIdx.y);
+  const int Zc0 = int(blockIdx.z) * ZB;
+  double acc = 0.0;
+  if (X < int(g.Mc1) && Y < int(g.Mc1)) {
+    const int F = int(g.Mf1) - 1;
+    int fx[3], fy[3];
+    T wx[3], wy[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int ox = 2 * X + d - 1, oy = 2 * Y + d - 1;
+      const T wd = d == 1 ? T(1) : T(0.5);
+      wx[d] = (ox < 0 || ox > F) ? T(0) : wd;
+      wy[d] = (oy < 0 || oy > F) ? T(0) : wd;
+      fx[d] = ox < 0 ? 0 : (ox > F ? F : ox);
+      fy[d] = oy < 0 ? 0 : (oy > F ? F : oy);
+    }
+    // fine planes 2*Zc0-1 .. 2*Zc0+2*ZB-1 (clamped), 9 values each
+    constexpr int NP = 2 * ZB + 1;
+    T v[NP][9];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      int oz = 2 * Zc0 - 1 + p;
+      oz = oz < 0 ? 0 : (oz > F ? F : oz);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const T* row = xf + (size_t(oz) * g.Mf1 + fy[b]) * g.Mf1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[p][b * 3 + c] = row[fx[c]];
+      }
+    }
+#pragma unroll
+    for (int zc = 0; zc < ZB; ++zc) {
+      const int Z = Zc0 + zc;
+      if (Z >= int(g.Mc1)) break;
+      T wz[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int oz = 2 * Z + d - 1;
+        wz[d] = (oz < 0 || oz > F) ? T(0) : (d == 1 ? T(1) : T(0.5));
+      }
+      T s = T(0);
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s += (wx[c] * wy[b] * wz[a]) * v[2 * zc + a][b * 3 + c];
+      const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
+      acc += epi(i, s);
+    }
+  }
+  const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const double blk = block_sum_tid<256>(acc, sh, tid);
+  const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
+  const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
 }
 
 }  // namespace fb

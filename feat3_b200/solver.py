@@ -20,7 +20,7 @@ STATUS = {0: "undefined", 1: "progress", 2: "success", 3: "aborted", 4: "diverge
 OUTER = {"pcg": 0, "richardson": 1}
 COARSE = {"direct": 0, "pcg": 1, "smoother": 2, "none": 3}
 PRECISION = {"f64": 0, "f32": 1, "f16": 2}
-FORMAT = {"sell": 0, "stencil": 1}
+FORMAT = {"sell": 0, "stencil": 1, "matfree": 2}
 RHS = {"sine": 0, "one": 1, "expbubble": 2}
 
 

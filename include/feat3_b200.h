@@ -32,6 +32,7 @@ extern "C" {
 #define FB_ERR_UNSUPPORTED 4  /* combination not implemented */
 #define FB_ERR_NOT_READY 5    /* object not initialised */
 #define FB_ERR_TOO_LARGE 6    /* request exceeds a fixed capacity of the entry point */
+#define FB_ERR_TIMEOUT 7      /* a bounded wait inside a kernel expired (the context stays usable) */
 
 #if defined(__GNUC__)
 #define FB_API __attribute__((visibility("default")))
@@ -197,9 +198,14 @@ FB_API void fb_mg_destroy(fb_mg* mg);
  *                     (what a hierarchy handed over by FEAT3 uses);
  *   FB_FORMAT_STENCIL on structured Q1 hierarchies: SELL-32 with implicit stencil columns
  *                     (no index stream) and matrix-free Q1 interpolation/restriction;
- *                     other hierarchies fall back to FB_FORMAT_SELL level by level. */
+ *                     other hierarchies fall back to FB_FORMAT_SELL level by level;
+ *   FB_FORMAT_MATFREE on structured Q1 hierarchies: no level matrix is read; every operator
+ *                     application (smoothers, defects, the outer solver's products) is formed
+ *                     from the per-cell coefficients and the reference element matrix, with
+ *                     matrix-free Q1 transfers; other hierarchies fall back as above. */
 #define FB_FORMAT_SELL 0
 #define FB_FORMAT_STENCIL 1
+#define FB_FORMAT_MATFREE 2
 typedef struct fb_solver_cfg {
   int outer;
   int nu;
@@ -211,7 +217,7 @@ typedef struct fb_solver_cfg {
   int max_iter;
   int precision;
   int use_graphs;     /* capture the per-iteration launch sequence in a CUDA graph */
-  int format;         /* FB_FORMAT_SELL or FB_FORMAT_STENCIL */
+  int format;         /* FB_FORMAT_SELL, FB_FORMAT_STENCIL or FB_FORMAT_MATFREE */
 } fb_solver_cfg;
 FB_API void fb_solver_cfg_default(fb_solver_cfg* cfg);
 FB_API int fb_mg_configure(fb_mg* mg, const fb_solver_cfg* cfg);

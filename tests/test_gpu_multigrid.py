@@ -37,7 +37,8 @@ CASES = [
 
 
 @pytest.mark.parametrize("case", CASES, ids=[f"d{c[0]}q{c[1]}L{c[2]}-{c[4]}-k{c[5]}-nu{c[6]}-{c[8]}" for c in CASES])
-@pytest.mark.parametrize("graphs,fmt", [(True, "sell"), (False, "sell"), (True, "stencil"), (False, "stencil")])
+@pytest.mark.parametrize("graphs,fmt", [(True, "sell"), (False, "sell"), (True, "stencil"), (False, "stencil"),
+                                        (True, "matfree"), (False, "matfree")])
 def test_structured_pcg_matches_oracle(case, graphs, fmt):
     from feat3_b200.solver import MultiGrid
     dim, deg, lvl, lmin, rhs, ks, nu, wj, coarse = case
@@ -109,7 +110,7 @@ def test_richardson_outer(outer, graphs):
 
 @pytest.mark.parametrize("prec", ["f32", "f16"])
 @pytest.mark.parametrize("outer", ["richardson", "pcg"])
-@pytest.mark.parametrize("fmt", ["sell", "stencil"])
+@pytest.mark.parametrize("fmt", ["sell", "stencil", "matfree"])
 def test_mixed_precision_error(prec, outer, fmt):
     from feat3_b200.solver import MultiGrid
     k = lognormal_k(3, 5, 1.0, seed=5)
@@ -147,7 +148,7 @@ def test_zero_rhs_and_nan_status():
     assert r["status"] == "aborted"
 
 
-@pytest.mark.parametrize("fmt", ["sell", "stencil"])
+@pytest.mark.parametrize("fmt", ["sell", "stencil", "matfree"])
 def test_vcycle_matches_oracle(fmt):
     from feat3_b200.solver import MultiGrid
     H = po.Hierarchy(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11))
