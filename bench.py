@@ -4,10 +4,11 @@
 k = exp(g), g ~ N(0,1) i.i.d., f = 1, homogeneous Dirichlet), one B200 per rank.
 
 One "step" is one complete solve from a zero initial guess to ||r|| <= 1e-8 ||r0|| with the
-hierarchy resident in HBM (5.5 GB finest-level matrix: every input is far larger than L2).
-  value  = mixed-precision solve time (FP64 outer PCG, FP32 V-cycle, FP16 matrix values)
+hierarchy resident in HBM (every finest-level operator application streams more than L2 holds).
+  value  = mixed-precision solve time (FP64 outer PCG, FP32 V-cycle, matrix-free Q1 operator)
   e2e    = the same solve through fb_mg_solve_host with pinned host rhs/solution buffers
-  fp64   = the plain FP64 GPU MG-PCG (the drop-in) on the same problem
+  fp64   = the plain FP64 GPU MG-PCG (the drop-in, assembled SELL matrices) on the same problem;
+           fp64_stencil / fp64_matfree: the FP64 solve on the other storage forms
 Multi-GPU: replicas only (each rank solves its own copy; no collective on the data path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--level L] [--impl reference]
@@ -28,6 +29,25 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-rel-1e-8 (mixed vs FP64 MG-PCG, 1 B200); SpMV HBM GB/s vs 8 TB/s"
+# headline form: FP64 outer PCG around an FP32 V-cycle on the matrix-free operator
+HEAD_PREC, HEAD_FMT = "f32", "matfree"
+HEAD_KERNEL = "matfree_jacobi_f32"
+HEAD_KERNEL_NAME = "k_mf_q1_tiled<float, EpiJacobi<float,0>> finest level (matrix-free Q1, bulk-copy staged)"
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from its committed ncu summary (profiles/<kernel>_*.md,
+    line 'dram_bytes_per_launch: N'), or None when no capture has been summarised."""
+    import glob
+    for fn in sorted(glob.glob(os.path.join(ROOT, "profiles", kernel + "_*.md"))):
+        with open(fn) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    try:
+                        return float(line.split(":", 1)[1].split()[0])
+                    except ValueError:
+                        return None
+    return None
 
 
 def parse():
@@ -49,7 +69,8 @@ def workload(level):
     n = (2 ** level + 1) ** 3
     return {"workload": f"3D Q1 Poisson, unit cube, {2 ** level}^3 cells ({n:,} DOFs), k=exp(N(0,1)) per element, "
                         f"f=1, Dirichlet 0; PCG + MG V(2,2) Richardson-Jacobi(0.5), levels 1..{level}, direct coarse",
-            "dofs": n, "level": level, "l2": "inputs larger than L2 (finest matrix alone 5.5 GB at level 8)"}
+            "dofs": n, "level": level, "l2": "inputs larger than L2 (126 MB): a finest-level matrix-free FP32 smoothing step streams "
+                  "~340 MB (x, k, rhs, 1/diag, result) at level 8; the assembled FP64 matrix is 5.5 GB"}
 
 
 def coefficient(level, seed):
@@ -218,50 +239,59 @@ def native_arm(args):
                               "dofs": n, "level": level}))
         mg.close()
         return 0
-    # --- FP64 forms: the drop-in (SELL-C-sigma, CSR transfers) and the same on the stencil storage
-    r64, t64, l64, it64, _ = run_form("f64", args.steps, args.warmup, fmt="sell")
+    # --- FP64 forms: the drop-in (SELL-C-sigma, CSR transfers), the stencil storage, matrix-free
+    r64, t64, _, it64, _ = run_form("f64", args.steps, args.warmup, fmt="sell")
     u64 = r64["u"].clone()
     r64s, t64s, _, it64s, _ = run_form("f64", args.steps, args.warmup, fmt="stencil")
-    # --- mixed form (headline)
+    r64m, t64m, _, it64m, _ = run_form("f64", args.steps, args.warmup, fmt=HEAD_FMT)
+    # --- mixed forms: FP16 stencil storage, and the headline (matrix-free FP32 V-cycle)
+    rmxs, tmxs, _, itmxs, _ = run_form("f16", args.steps, args.warmup, fmt="stencil")
+    err_s = float(torch.linalg.norm(rmxs["u"] - u64) / torch.linalg.norm(u64))
     clk = ClockSampler(local)
     clk.start()
-    rmx, tmx, lmx, itmx, wall = run_form("f16", args.steps, args.warmup, fmt="stencil")
+    rmx, tmx, lmx, itmx, wall = run_form(HEAD_PREC, args.steps, args.warmup, fmt=HEAD_FMT)
     clocks = clk.stop()
     umx = rmx["u"]
     err = float(torch.linalg.norm(umx - u64) / torch.linalg.norm(u64))
     # --- one adjoint gradient solve on the same hierarchy (transposed MG-PCG + element gradient)
     u_target = (0.9 * umx).contiguous()
     adj = {}
-    for prec in ("f16", "f64"):
-        mg.configure(precision=prec, format="stencil", **common)
+    for prec in (HEAD_PREC, "f64"):
+        mg.configure(precision=prec, format=HEAD_FMT, **common)
         mg.adjoint_grad(umx, u_target)  # warm-up
         torch.cuda.synchronize()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         lam, grad, ainfo = mg.adjoint_grad(umx, u_target)
         torch.cuda.synchronize()
         adj[prec] = {"time_s": time.perf_counter() - t0, "solve_s": ainfo["solve_ms"] / 1e3, "iters": ainfo["iters"],
                      "status": ainfo["status"], "grad_norm": float(torch.linalg.norm(grad))}
         adj[prec + "_grad"] = grad
-    adj_err = float(torch.linalg.norm(adj["f16_grad"] - adj["f64_grad"]) / torch.linalg.norm(adj["f64_grad"]))
-    adjoint = {"mixed": adj["f16"], "fp64": adj["f64"], "grad_rel_diff_mixed_vs_fp64": adj_err,
+    adj_err = float(torch.linalg.norm(adj[HEAD_PREC + "_grad"] - adj["f64_grad"]) / torch.linalg.norm(adj["f64_grad"]))
+    adjoint = {"mixed": adj[HEAD_PREC], "fp64": adj["f64"], "grad_rel_diff_mixed_vs_fp64": adj_err,
                "objective": "J = 1/2 ||u - u_t||^2, u_t = 0.9 u"}
     # --- end to end through the host-buffer entry point
-    re2e, te2e, _, _, _ = run_form("f16", max(2, args.steps // 2), 1, host=True, fmt="stencil")
+    re2e, te2e, _, _, _ = run_form(HEAD_PREC, max(2, args.steps // 2), 1, host=True, fmt=HEAD_FMT)
 
-    # --- roofline of the finest-level SpMV kernels (CUDA events on the solver stream)
+    # --- roofline of the finest-level operator kernels (CUDA events on the solver stream)
     nnz = mg.nnz(0)
+    ne = (2 ** level) ** 3
     rf = {}
-    for name, prec, fmt, which, sv, si, sx in (
-            ("stencil_jacobi_f16", "f16", "stencil", 0, 2, 0, 4), ("stencil_jacobi_f64", "f64", "stencil", 0, 8, 0, 8),
-            ("stencil_pcgq_f64", "f64", "stencil", 2, 8, 0, 8), ("sell_jacobi_f64", "f64", "sell", 0, 8, 4, 8),
-            ("sell_pcgq_f64", "f64", "sell", 2, 8, 4, 8), ("sell_jacobi_f16", "f16", "sell", 0, 2, 4, 4)):
+    for name, prec, fmt, which in (
+            ("matfree_jacobi_f32", "f32", "matfree", 0), ("matfree_pcgq_f64", "f64", "matfree", 2),
+            ("stencil_jacobi_f16", "f16", "stencil", 0), ("stencil_jacobi_f64", "f64", "stencil", 0),
+            ("stencil_pcgq_f64", "f64", "stencil", 2), ("sell_jacobi_f64", "f64", "sell", 0),
+            ("sell_pcgq_f64", "f64", "sell", 2), ("sell_jacobi_f16", "f16", "sell", 0)):
         mg.configure(precision=prec, format=fmt, **common)
         ms = C.c_double(0.0)
         _lib.call("fb_mg_time_spmv", mg.h, 0, which, {"f64": 0, "f32": 1, "f16": 2}[prec], 20, C.byref(ms))
-        # algorithmic bytes: nnz*(value + index) + x once + the row streams of the epilogue + mask
-        vec = n * sx * (3 if which == 0 else 2)  # Jacobi: rhs, invd, out; PCG q: p (own row), q
-        alg = nnz * (sv + si) + n * sx + vec + n / 8
+        sx = 8 if prec == "f64" else 4                    # vector element size
+        vec = n * sx * (3 if which == 0 else 1)           # Jacobi: rhs, invd, out; PCG q: q (p is the input)
+        if fmt == "matfree":
+            mat = ne * sx                                 # per-cell coefficient instead of a matrix
+        else:
+            sv = {"f64": 8, "f32": 4, "f16": 2}[prec]
+            mat = nnz * (sv + (4 if fmt == "sell" else 0))  # values (+ 32-bit column indices)
+        alg = mat + n * sx + vec + n / 8                  # + the input vector once + the filter mask
         rf[name] = {"ms": ms.value, "bytes": alg, "GBps": alg / (ms.value * 1e-3) / 1e9}
     peaks = {}
     try:
@@ -270,11 +300,13 @@ def native_arm(args):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    dom = rf["stencil_jacobi_f16"]
+    dom = rf[HEAD_KERNEL]
 
     t_mixed = max_over_ranks(float(np.median(tmx)))
+    t_mixed_s = max_over_ranks(float(np.median(tmxs)))
     t_fp64 = max_over_ranks(float(np.median(t64)))
     t_fp64s = max_over_ranks(float(np.median(t64s)))
+    t_fp64m = max_over_ranks(float(np.median(t64m)))
     t_e2e = max_over_ranks(float(np.median(te2e)))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -285,21 +317,27 @@ def native_arm(args):
         line = {
             "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 outer / f32 V-cycle / f16 matrix storage", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64 outer PCG / f32 V-cycle (matrix-free operator)", "data": "synthetic",
             "config": {**workload(level), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "seed": args.seed},
             "mixed": {"time_s": t_mixed, "iters": itmx[-1], "err_vs_fp64": err,
-                      "dof_it_per_s": n * itmx[-1] / t_mixed, "final_rel_residual": rmx["hist"][-1] / rmx["hist"][0]},
+                      "dof_it_per_s": n * itmx[-1] / t_mixed, "final_rel_residual": rmx["hist"][-1] / rmx["hist"][0],
+                      "storage": "matrix-free Q1 operator from per-cell coefficients + matrix-free Q1 transfers"},
+            "mixed_f16_stencil": {"time_s": t_mixed_s, "iters": itmxs[-1], "err_vs_fp64": err_s,
+                                  "storage": "FP16 stencil values (SELL-32, implicit columns) + matrix-free transfers"},
             "fp64": {"time_s": t_fp64, "iters": it64[-1], "dof_it_per_s": n * it64[-1] / t_fp64,
                      "final_rel_residual": r64["hist"][-1] / r64["hist"][0],
                      "storage": "SELL-C-sigma (C=32, 32-bit column indices) + CSR transfers (drop-in form)"},
             "fp64_stencil": {"time_s": t_fp64s, "iters": it64s[-1], "dof_it_per_s": n * it64s[-1] / t_fp64s,
                              "storage": "SELL-32 with implicit stencil columns + matrix-free Q1 transfers"},
+            "fp64_matfree": {"time_s": t_fp64m, "iters": it64m[-1], "dof_it_per_s": n * it64m[-1] / t_fp64m,
+                             "storage": "matrix-free Q1 operator + matrix-free Q1 transfers"},
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
-            "speedup_mixed_vs_fp64_same_storage": t_fp64s / t_mixed,
+            "speedup_mixed_vs_fp64_same_storage": t_fp64m / t_mixed,
             "roofline": {"bound": "hbm", "achieved": dom["GBps"], "peak": peak, "unit": "GB/s",
-                         "frac": dom["GBps"] / peak, "traffic": None, "kernel": "k_stencil<__half,float,float,EpiJacobi,27> finest level (FP16 values, implicit columns)",
-                         "kernels": rf, "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650"},
+                         "frac": dom["GBps"] / peak, "traffic": profiled_traffic(HEAD_KERNEL),
+                         "kernel": HEAD_KERNEL_NAME, "kernels": rf,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650"},
             "adjoint": adjoint,
             "cpu_baseline": cpu,
             "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},

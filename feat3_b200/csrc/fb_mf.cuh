@@ -7,7 +7,9 @@
 // Z-1, Z; cell lines Y0-1..Y0+Lt-1) and one range per streamed epilogue vector (the tile's
 // own lines). One producer warp copies those ranges into an NST-deep ring of stage buffers
 // (each range widened to 16-byte boundaries, which the padded allocations of the driver
-// allow); eight consumer warps compute one row per thread from shared memory. Rows outside
+// allow); eight consumer warps compute TY rows per thread from shared memory, walking up a
+// line column with a sliding window (9 new x values and 4 new cell coefficients per row,
+// the other 18 + 4 are kept in registers). Rows outside
 // the tiles (the lattice boundary planes and lines and the two ends of interior lines) are
 // formed afterwards by the same warps with direct loads.
 //
@@ -31,14 +33,15 @@ struct Staged<EpiJacobi<T, RED>> {
   static constexpr int kStreams = 2;
   static const void* stream(const E& e, int i) { return i == 0 ? (const void*)e.rhs : (const void*)e.invd; }
   static bool input_is_x(const E& e, const void* x) { return e.x == x; }
+  static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E& e) { return smoother_skip<T>(e.skip_src); }
-  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st) {
+  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st, bool m) {
     if (skp) {
       e.out[row] = e.s0 ? e.s0[row] : T(0);
       return 0.0;
     }
     const T d = st[0] - s;
-    if (masked(e.mask, row)) {
+    if (m) {
       e.out[row] = xc;
       return 0.0;
     }
@@ -55,10 +58,11 @@ struct Staged<EpiDefect<T, RED, LOW>> {
   static constexpr int kStreams = 1;
   static const void* stream(const E& e, int) { return e.rhs; }
   static bool input_is_x(const E&, const void*) { return true; }
+  static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E&) { return false; }
-  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T, const T* st) {
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T, const T* st, bool m) {
     T d = st[0] - s;
-    if (masked(e.mask, row)) d = T(0);
+    if (m) d = T(0);
     e.def[row] = d;
     if (LOW) e.def32[row] = float(d);
     return RED ? double(d) * double(d) : 0.0;
@@ -72,32 +76,47 @@ struct Staged<EpiPcgQ<T>> {
   static constexpr int kStreams = 0;
   static const void* stream(const E&, int) { return nullptr; }
   static bool input_is_x(const E& e, const void* x) { return e.p == x; }  // q . p with p the product's input
+  static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E&) { return false; }
-  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T xc, const T*) {
-    const T v = masked(e.mask, row) ? T(0) : s;
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T xc, const T*, bool m) {
+    const T v = m ? T(0) : s;
     e.q[row] = v;
     return double(v) * double(xc);
   }
 };
 
 // ------------------------------------------------------------------ tile geometry
+// A tile holds Lt = G * TY consecutive interior lines of one interior plane: G groups of W
+// threads (W = M1 - 2, one thread per interior point of a line), each group walking TY
+// consecutive lines with a sliding register window.
 struct MfTile {
   uint32_t M1, N;        // lattice points and cells per side
-  uint32_t Lt, tpp;      // lines per tile, tiles per interior plane
+  uint32_t G, Lt, tpp;   // thread groups, lines per tile (G * TY), tiles per interior plane
   uint32_t ntiles;       // (M1 - 2) * tpp
-  uint32_t cap_x, cap_k, cap_s;  // bytes reserved per x / k / stream range in a stage
+  uint32_t cap_x, cap_k, cap_s, cap_m;  // bytes reserved per x / k / stream / mask range in a stage
   uint32_t stage_bytes;
   uint32_t nbl_items;    // direct-path items: boundary-line chunks
   uint32_t nedge_items;  // direct-path items: 16 interior lines' end points each
+  uint32_t dz, dyt;      // grid stride in tiles, as (planes, tiles within a plane) = divmod(gridDim, tpp)
 };
 
+// tiles of a block in grid-stride order without divisions in the loop
+struct TileIter {
+  uint32_t Z, yt;  // plane (1-based interior plane index) and tile within the plane
+  __device__ __forceinline__ TileIter(const MfTile& G, uint32_t t0) : Z(1 + t0 / G.tpp), yt(t0 % G.tpp) {}
+  __device__ __forceinline__ void next(const MfTile& G) {
+    yt += G.dyt;
+    Z += G.dz;
+    if (yt >= G.tpp) { yt -= G.tpp; ++Z; }
+  }
+};
 struct TileGeo {
   uint32_t Z, Y0, lt;
 };
-__device__ __forceinline__ TileGeo tile_geo(const MfTile& G, uint32_t t) {
+__device__ __forceinline__ TileGeo tile_geo(const MfTile& G, const TileIter& ti) {
   TileGeo g;
-  g.Z = 1 + t / G.tpp;
-  g.Y0 = 1 + (t % G.tpp) * G.Lt;
+  g.Z = ti.Z;
+  g.Y0 = 1 + ti.yt * G.Lt;
   const uint32_t rem = G.M1 - 1 - g.Y0;  // interior lines left in the plane
   g.lt = rem < G.Lt ? rem : G.Lt;
   return g;
@@ -190,12 +209,14 @@ __device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __res
 
 // ------------------------------------------------------------------ the tiled kernel
 // 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
-template<typename T, typename Epi, int NST, int MINB>
+template<typename T, typename Epi, int NST, int MINB, int TY>
 __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTile G, const T* __restrict__ x, Epi epi,
-                                                           const T* st0, const T* st1, double* ws, unsigned* counter,
-                                                           double* red_out, unsigned* kerr) {
+                                                           const T* st0, const T* st1, const uint32_t* mask,
+                                                           double* ws, unsigned* counter, double* red_out,
+                                                           unsigned* kerr) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
+  constexpr uint64_t E = 16 / sizeof(T);
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[NST], empty[NST];
   __shared__ double sh[16];
@@ -210,56 +231,82 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
   __syncthreads();
   const uint32_t M1 = G.M1, N = G.N;
   const uint32_t W = M1 - 2;  // interior points per line
+  // stage layout: x planes | k cell planes | streams | mask words
+  const uint32_t off_k = 3 * G.cap_x, off_s = off_k + 2 * G.cap_k, off_m = off_s + NS * G.cap_s;
   double acc = 0.0;
   if (warp == 8) {
-    // ---------------- producer
-    if (lane == 0) {
-      uint32_t it = 0;
-      for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it) {
-        const int s = int(it % NST);
-        const uint32_t ph = (it / NST) & 1u;
-        if (it >= NST && !mbar_wait(&empty[s], ph ^ 1u)) {
-          atomicExch(kerr, 1u);
+    // ---------------- producer: lane q computes and issues copy q of the tile
+    // (0-2: x planes, 3-4: cell planes, 5-6: streams, 7: mask words)
+    uint32_t it = 0;
+    bool stop = false;
+    TileIter ti(G, blockIdx.x);
+    for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it, ti.next(G)) {
+      const int s = int(it % NST);
+      const uint32_t ph = (it / NST) & 1u;
+      if (it >= NST) {
+        const bool okw = lane == 0 ? mbar_wait(&empty[s], ph ^ 1u) : true;
+        if (!__shfl_sync(0xffffffffu, okw, 0)) {
+          if (lane == 0) atomicExch(kerr, 1u);
+          stop = true;
           break;
         }
-        const TileGeo g = tile_geo(G, t);
-        unsigned char* st = smem + size_t(s) * G.stage_bytes;
-        uint64_t lo[6];
-        uint32_t by[6];
-        uint32_t total = 0;
-        for (int q = 0; q < 3; ++q) {
-          const uint64_t zp = g.Z - 1 + q;
-          widen<T>((zp * M1 + g.Y0 - 1) * M1, (zp * M1 + g.Y0 + g.lt) * M1 + M1 - 1, lo[q], by[q]);
-          total += by[q];
-        }
-        for (int q = 0; q < 2 && A.k; ++q) {
-          const uint64_t ez = g.Z - 1 + q;
-          widen<T>((ez * N + g.Y0 - 1) * N, (ez * N + g.Y0 + g.lt - 1) * N + N - 1, lo[3 + q], by[3 + q]);
-          total += by[3 + q];
-        }
-        if (NS > 0) {
-          widen<T>((uint64_t(g.Z) * M1 + g.Y0) * M1, (uint64_t(g.Z) * M1 + g.Y0 + g.lt - 1) * M1 + M1 - 1, lo[5], by[5]);
-          total += NS * by[5];
-        }
-        mbar_arrive_tx(&full[s], total);
-        for (int q = 0; q < 3; ++q) bulk_g2s(st + q * G.cap_x, x + lo[q], by[q], &full[s]);
-        for (int q = 0; q < 2 && A.k; ++q) bulk_g2s(st + 3 * G.cap_x + q * G.cap_k, A.k + lo[3 + q], by[3 + q], &full[s]);
-        if (NS > 0) bulk_g2s(st + 3 * G.cap_x + 2 * G.cap_k, st0 + lo[5], by[5], &full[s]);
-        if (NS > 1) bulk_g2s(st + 3 * G.cap_x + 2 * G.cap_k + G.cap_s, st1 + lo[5], by[5], &full[s]);
       }
-      // copies still in flight (none unless the consumers stopped early)
+      const TileGeo g = tile_geo(G, ti);
+      unsigned char* st = smem + size_t(s) * G.stage_bytes;
+      const uint64_t r0 = (uint64_t(g.Z) * M1 + g.Y0) * M1, r1 = r0 + uint64_t(g.lt) * M1 - 1;
+      uint64_t lo = 0;
+      uint32_t by = 0, dst = 0;
+      const void* src = nullptr;
+      if (lane < 3) {
+        const uint64_t zp = g.Z - 1 + lane;
+        widen<T>((zp * M1 + g.Y0 - 1) * M1, (zp * M1 + g.Y0 + g.lt) * M1 + M1 - 1, lo, by);
+        src = x + lo;
+        dst = lane * G.cap_x;
+      } else if (lane < 5) {
+        if (A.k) {
+          const uint64_t ez = g.Z - 1 + (lane - 3);
+          widen<T>((ez * N + g.Y0 - 1) * N, (ez * N + g.Y0 + g.lt - 1) * N + N - 1, lo, by);
+          src = A.k + lo;
+          dst = off_k + (lane - 3) * G.cap_k;
+        }
+      } else if (lane < 7) {
+        if (lane - 5 < NS) {
+          widen<T>(r0, r1, lo, by);
+          src = (lane == 5 ? st0 : st1) + lo;
+          dst = off_s + (lane - 5) * G.cap_s;
+        }
+      } else if (lane == 7) {
+        if (mask) {
+          widen<uint32_t>(r0 >> 5, r1 >> 5, lo, by);
+          src = mask + lo;
+          dst = off_m;
+        }
+      }
+      uint32_t total = by;
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+      if (lane == 0) mbar_arrive_tx(&full[s], total);
+      __syncwarp();
+      if (by) bulk_g2s(st + dst, src, by, &full[s]);
+    }
+    // copies still in flight (none unless the consumers stopped early)
+    (void)stop;
+    if (lane == 0) {
       const uint32_t issued = it;
       for (uint32_t j = issued > NST ? issued - NST : 0; j < issued; ++j)
         if (!mbar_wait(&full[j % NST], (j / NST) & 1u)) atomicExch(kerr, 2u);
     }
     __syncwarp();
   } else {
-    // ---------------- consumers: one row per thread and tile
+    // ---------------- consumers: TY rows per thread and tile (sliding window along Y)
     const bool skp = SE::skip(epi);
     const uint32_t tid = threadIdx.x;
+    const uint32_t grp = tid / W, X = 1 + (tid - grp * W);
+    const bool active = grp < G.G;
     uint32_t it = 0;
     bool ok = true;
-    for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it) {
+    TileIter ti(G, blockIdx.x);
+    for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it, ti.next(G)) {
       const int s = int(it % NST);
       const uint32_t ph = (it / NST) & 1u;
       if (!mbar_wait(&full[s], ph)) {
@@ -267,63 +314,87 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
         ok = false;
         break;
       }
-      const TileGeo g = tile_geo(G, t);
+      const TileGeo g = tile_geo(G, ti);
       const unsigned char* st = smem + size_t(s) * G.stage_bytes;
-      if (tid < g.lt * W) {
-        const uint32_t ly = tid / W, X = 1 + tid % W;
-        constexpr uint64_t E = 16 / sizeof(T);
+      const uint32_t l0 = grp * TY;  // first line of this group, relative to Y0
+      if (active && l0 < g.lt) {
+        // window origin: x line Y0-1+l0 of each plane, k cell line Y0-1+l0, at this X
         const T* xs[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           const uint64_t zp = g.Z - 1 + q;
-          const uint64_t l0 = (zp * M1 + g.Y0 - 1) * M1;
-          xs[q] = reinterpret_cast<const T*>(st + q * G.cap_x) + (l0 & (E - 1)) + (ly + 1) * M1 + X;
+          const uint64_t xlo = (zp * M1 + g.Y0 - 1) * M1;
+          xs[q] = reinterpret_cast<const T*>(st + q * G.cap_x) + (xlo & (E - 1)) + l0 * M1 + X;
         }
-        T xv[27];
-#pragma unroll
-        for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-          for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-            for (int dx = 0; dx < 3; ++dx) xv[dz * 9 + dy * 3 + dx] = xs[dz][(int(dy) - 1) * int(M1) + dx - 1];
-        T kv[8];
+        const T* ks[2] = {nullptr, nullptr};
         if (A.k) {
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const uint64_t ez = g.Z - 1 + q;
-            const uint64_t c0 = (ez * N + g.Y0 - 1) * N;
-            const T* ks = reinterpret_cast<const T*>(st + 3 * G.cap_x + q * G.cap_k) + (c0 & (E - 1)) + ly * N + (X - 1);
-            kv[q * 4 + 0] = ks[0];
-            kv[q * 4 + 1] = ks[1];
-            kv[q * 4 + 2] = ks[N];
-            kv[q * 4 + 3] = ks[N + 1];
+            const uint64_t klo = (ez * N + g.Y0 - 1) * N;
+            ks[q] = reinterpret_cast<const T*>(st + off_k + q * G.cap_k) + (klo & (E - 1)) + l0 * N + (X - 1);
           }
-        } else {
-#pragma unroll
-          for (int e = 0; e < 8; ++e) kv[e] = T(1);
         }
-        T s = T(0);
+        const uint32_t r0 = (g.Z * M1 + g.Y0) * M1;  // rows < 2^31 (checked by the launcher)
+        const T* ss = reinterpret_cast<const T*>(st + off_s) + (r0 & uint32_t(E - 1)) + l0 * M1 + X;
+        const uint32_t* ms = reinterpret_cast<const uint32_t*>(st + off_m);
+        const uint32_t mw0 = (r0 >> 5) & ~3u;  // first staged mask word
+        // window: xw[plane][line][dx], kw[cell plane][cell line][ex]
+        T xw[3][3][3], kw[2][2][2];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
-          const int a = (1 - ox) | ((1 - oy) << 1) | ((1 - oz) << 2);
-          T in = T(0);
+        for (int q = 0; q < 3; ++q)
 #pragma unroll
-          for (int b = 0; b < 8; ++b) {
-            const int dx = ox + (b & 1), dy = oy + ((b >> 1) & 1), dz = oz + ((b >> 2) & 1);
-            in += A.kr[a ^ b] * xv[dz * 9 + dy * 3 + dx];
+          for (int l = 0; l < 2; ++l)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) xw[q][l][d] = xs[q][l * int(M1) + d - 1];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          kw[q][0][0] = A.k ? ks[q][0] : T(1);
+          kw[q][0][1] = A.k ? ks[q][1] : T(1);
+        }
+#pragma unroll
+        for (int j = 0; j < TY; ++j) {
+          if (l0 + j >= g.lt) break;
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) xw[q][2][d] = xs[q][(j + 2) * int(M1) + d - 1];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            kw[q][1][0] = A.k ? ks[q][(j + 1) * N] : T(1);
+            kw[q][1][1] = A.k ? ks[q][(j + 1) * N + 1] : T(1);
           }
-          s += kv[oz * 4 + oy * 2 + ox] * in;
+          T s = T(0);
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
+            const int a = (1 - ox) | ((1 - oy) << 1) | ((1 - oz) << 2);
+            T in = T(0);
+#pragma unroll
+            for (int b = 0; b < 8; ++b)
+              in += A.kr[a ^ b] * xw[oz + ((b >> 2) & 1)][oy + ((b >> 1) & 1)][ox + (b & 1)];
+            s += kw[oz][oy][ox] * in;
+          }
+          const uint32_t row = r0 + (l0 + j) * M1 + X;
+          T sv[NS > 0 ? NS : 1];
+          if (NS > 0) sv[0] = ss[j * int(M1)];
+          if (NS > 1) sv[NS > 1 ? 1 : 0] = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[j * int(M1)];
+          const bool mb = mask ? ((ms[(row >> 5) - mw0] >> (row & 31)) & 1u) : false;
+          acc += SE::apply(epi, skp, row, s, xw[1][1][1], sv, mb);
+          // slide the window one line up
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              xw[q][0][d] = xw[q][1][d];
+              xw[q][1][d] = xw[q][2][d];
+            }
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            kw[q][0][0] = kw[q][1][0];
+            kw[q][0][1] = kw[q][1][1];
+          }
         }
-        const uint32_t row = (g.Z * M1 + g.Y0 + ly) * M1 + X;
-        T sv[NS > 0 ? NS : 1];
-        if (NS > 0) {
-          const uint64_t r0 = (uint64_t(g.Z) * M1 + g.Y0) * M1;
-          const T* ss = reinterpret_cast<const T*>(st + 3 * G.cap_x + 2 * G.cap_k) + (r0 & (E - 1)) + ly * M1 + X;
-          sv[0] = ss[0];
-          if (NS > 1) sv[NS > 1 ? 1 : 0] = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[0];
-        }
-        acc += SE::apply(epi, skp, row, s, xv[13], sv);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);

@@ -17,6 +17,7 @@
 //     the norm is reduced inside the kernel that produces the defect and read by the next.
 #include "fb_mg_internal.cuh"
 #include "fb_mf.cuh"
+#include "fb_coarse.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __res
   }
 }
 
-// PCG update: alpha = gamma / qp; x += alpha p; r -= alpha q; ||r||^2 (+ FP32 copy of r)
+// PCG update: alpha = rz / qp; x += alpha p; r -= alpha q; ||r||^2 (+ FP32 copy of r)
 // (pcg.hpp:241-251 with the |alpha| < eps shortcut of dense_vector.hpp:891-895)
 // When s1 != nullptr the kernel also forms the first pre-smoothing step of the next V-cycle
 // from zero, s1 = omega * filter_cor(invd o r) in the V-cycle's type (k_jacobi0 on the new r;
@@ -237,12 +238,14 @@ __global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __res
 // restored by the second step, which sees the same skip test).
 template<bool LOW>
 __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float* r32, const double* __restrict__ p,
-                                                    const double* __restrict__ q, const DevScalars* sc, uint32_t n,
+                                                    const double* __restrict__ q, DevScalars* sc, uint32_t n,
                                                     double* ws, unsigned* counter, double* rr_out,
                                                     void* s1, const void* invd, const uint32_t* mask, double omega) {
   using T = typename std::conditional<LOW, float, double>::type;
   __shared__ double sh[8];
-  const double alpha = sc->gamma / sc->qp;
+  // alpha = gamma' / (q . p) with gamma' = r . z of this iteration (pcg.hpp:241-251); the thread
+  // that finishes the reduction then commits gamma <- gamma' for the next direction update
+  const double alpha = sc->rz / sc->qp;
   const bool upd = fabs(alpha) >= eps_of<double>();
   T* s1t = static_cast<T*>(s1);
   const T* invt = static_cast<const T*>(invd);
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
     acc += ri * ri;
   }
   const double blk = block_sum<256>(acc, sh);
-  reduce_finish<256>(blk, ws, counter, rr_out, sh, false);
+  if (reduce_finish<256>(blk, ws, counter, rr_out, sh, false)) sc->gamma = sc->rz;
 }
 
 // r . z with z in FP64 or FP32 (ConvertPrecond: z = double(z_inner))
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
   reduce_finish<256>(blk, ws, counter, out, sh, false);
 }
 
-// p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is done by the next kernel
+// p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update
 template<typename ZT>
 __global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
   const double beta = sc->rz / sc->gamma;
@@ -284,7 +287,6 @@ __global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars*
     p[i] = upd ? beta * p[i] + double(z[i]) : double(z[i]);
 }
 
-__global__ void k_commit_gamma(DevScalars* sc) { sc->gamma = sc->rz; }
 __global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; }
 
 // Richardson outer: x = omega * z + x
@@ -383,23 +385,27 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
                            double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
-  constexpr int NST = sizeof(T) == 4 ? 4 : 3;
+  constexpr int NST = 2;
   constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
+  constexpr int TY = sizeof(T) == 4 ? 4 : 2;
   const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
+  const uint32_t* mask = SE::mask(epi);
   MfTile G;
   G.M1 = M1; G.N = N;
-  G.Lt = std::max<uint32_t>(1, 256 / W);
+  G.G = std::max<uint32_t>(1, 256 / W);
+  G.Lt = G.G * TY;
   G.tpp = (W + G.Lt - 1) / G.Lt;
   G.ntiles = W * G.tpp;
   G.cap_x = r16(uint64_t(G.Lt + 2) * M1 * sizeof(T)) + 32;
   G.cap_k = v.k ? r16(uint64_t(G.Lt + 1) * N * sizeof(T)) + 32 : 0;
   G.cap_s = NS ? r16(uint64_t(G.Lt) * M1 * sizeof(T)) + 32 : 0;
-  G.stage_bytes = (3 * G.cap_x + 2 * G.cap_k + NS * G.cap_s + 127) & ~127u;
+  G.cap_m = mask ? r16((uint64_t(G.Lt) * M1 / 32 + 2) * 4) + 32 : 0;
+  G.stage_bytes = (3 * G.cap_x + 2 * G.cap_k + NS * G.cap_s + G.cap_m + 127) & ~127u;
   G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
   G.nedge_items = (W * W + 15) / 16;
   const size_t dyn = size_t(NST) * G.stage_bytes;
-  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB>;
+  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
   if (dyn > attr) {
     FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
@@ -411,9 +417,11 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
     bps = 1;
   }
   const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(G.ntiles, uint32_t(bps) * kSMs));
+  G.dz = grid / G.tpp;
+  G.dyt = grid % G.tpp;
   const T* s0 = NS > 0 ? static_cast<const T*>(SE::stream(epi, 0)) : nullptr;
   const T* s1 = NS > 1 ? static_cast<const T*>(SE::stream(epi, 1)) : nullptr;
-  fn<<<grid, 288, dyn, m->stream>>>(v, G, x, epi, s0, s1, m->ws, m->counter, red_out, m->kerr);
+  fn<<<grid, 288, dyn, m->stream>>>(v, G, x, epi, s0, s1, mask, m->ws, m->counter, red_out, m->kerr);
   m->launches++;
   FB_CHECK_LAUNCH();
   return FB_OK;
@@ -433,7 +441,8 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   }
   for (int j = 0; j < (DIM == 3 ? 27 : 9); ++j) v.off[j] = L.St.off[j];
   if constexpr (DIM == 3 && Staged<Epi>::kOk) {
-    if (L.M1 >= 18 && Staged<Epi>::input_is_x(epi, x) && !v.err) return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
+    if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err)
+      return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
   }
   auto fn = k_mf_q1<T, Epi, DIM>;
   if (debug_enabled())
@@ -539,14 +548,112 @@ static int presmooth(fb_mg* m, int l, const T* b, const double* bnorm, bool need
   return FB_OK;
 }
 
+// ------------------------------------------------------------------ fused coarse cycle
+constexpr uint32_t kCoarseRows = 40000;  // levels up to this size go to the one-cluster kernel
+constexpr int kCoarseThreads = 512;
+
+template<typename T, int DIM>
+static int coarse_cluster_size(fb_mg* m) {
+  // largest cluster (16 non-portable, else 8) that the device can schedule for the kernel
+  static int cs = -1;
+  if (cs >= 0) return cs;
+  cs = 0;
+  auto fn = k_coarse_cycle<T, DIM, kCoarseThreads>;
+  (void)m;
+  for (int want : {16, 8}) {
+    if (want > 8 && cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(want);
+    cfg.blockDim = dim3(kCoarseThreads);
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = want; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, (const void*)fn, &cfg) == cudaSuccess && nc > 0) { cs = want; break; }
+    cudaGetLastError();
+  }
+  return cs;
+}
+
+// first level of the fused coarse cycle, or nl when the coarse end runs level by level
+template<typename T>
+static int coarse_start(fb_mg* m) {
+  const int nl = (int)m->L.size();
+  if (m->cfg.format != FB_FORMAT_MATFREE || m->cfg.coarse == FB_COARSE_PCG || !m->coarse_fuse) return nl;
+  int lc = nl;
+  for (int l = nl - 1; l >= 1; --l) {
+    if (!m->L[l].mf || m->L[l].n > kCoarseRows) break;
+    lc = l;
+  }
+  if (nl - lc < 2 || nl - lc > kCoarseMax) return nl;
+  const int cs = m->dim == 3 ? coarse_cluster_size<T, 3>(m) : coarse_cluster_size<T, 2>(m);
+  return cs > 0 ? lc : nl;
+}
+
+template<typename T>
+static int launch_coarse(fb_mg* m, int lc, T** sol_lc) {
+  const int nl = (int)m->L.size();
+  CoarseArgs<T> A;
+  A.nlv = nl - lc;
+  A.nu = m->cfg.nu;
+  A.coarse = m->cfg.coarse;
+  A.omega = T(m->cfg.omega_rich);
+  if constexpr (std::is_same<T, double>::value) A.cinv = m->cinv64; else A.cinv = m->cinv32;
+  A.red = m->cred;
+  A.s1_coarsest = m->cfg.coarse == FB_COARSE_SMOOTHER ? 1 : 0;
+  for (int i = 0; i < A.nlv; ++i) {
+    Level& L = m->L[lc + i];
+    CLevel<T>& c = A.L[i];
+    c.n = L.n; c.M1 = L.M1;
+    if constexpr (std::is_same<T, double>::value) {
+      c.k = L.k;
+      for (int r = 0; r < 8; ++r) c.kr[r] = L.kr64[r];
+    } else {
+      c.k = L.k ? L.k32 : nullptr;
+      for (int r = 0; r < 8; ++r) c.kr[r] = L.kr32[r];
+    }
+    c.mask = L.mask; c.invd = Prec<T>::invd(L);
+    c.rhs = Prec<T>::rhs(L); c.x = Prec<T>::x(L); c.y = Prec<T>::y(L); c.def = Prec<T>::def(L);
+    c.bn = &m->sc->lvl[2 * (lc + i)];
+    c.dn = &m->sc->lvl[2 * (lc + i) + 1];
+  }
+  const int cs = m->dim == 3 ? coarse_cluster_size<T, 3>(m) : coarse_cluster_size<T, 2>(m);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = dim3(kCoarseThreads);
+  cfg.stream = m->stream;
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeClusterDimension;
+  at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  if (m->dim == 3) FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 3, kCoarseThreads>, A));
+  else FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 2, kCoarseThreads>, A));
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  // the kernel's pointer walk: nu - 1 swaps in the pre-smoothing of level lc, nu in its post-smoothing
+  Level& L = m->L[lc];
+  T* cur = Prec<T>::x(L);
+  for (int it = 1; it < m->cfg.nu; ++it) cur = (cur == Prec<T>::x(L)) ? Prec<T>::y(L) : Prec<T>::x(L);
+  for (int it = 0; it < m->cfg.nu; ++it) cur = (cur == Prec<T>::x(L)) ? Prec<T>::y(L) : Prec<T>::x(L);
+  *sol_lc = cur;
+  return FB_OK;
+}
+
 template<typename T>
 static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** out_top) {
   const int nl = (int)m->L.size();
   const int nu = m->cfg.nu;
   const T omega = T(m->cfg.omega_rich);
   std::vector<T*> sol(nl, nullptr);
+  const int lc = coarse_start<T>(m);
   // ---- descent (multigrid.hpp:1711-1832)
-  for (int l = 0; l + 1 < nl; ++l) {
+  for (int l = 0; l + 1 < nl && l < lc; ++l) {
     Level& L = m->L[l];
     Level& C = m->L[l + 1];
     const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
@@ -562,7 +669,9 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     FB_TRY(rest_T<T>(m, l, Prec<T>::def(L), er, &m->sc->lvl[2 * (l + 1)]));
   }
   // ---- coarse grid (multigrid.hpp:1524-1587)
-  {
+  if (lc < nl) {
+    FB_TRY(launch_coarse<T>(m, lc, &sol[lc]));
+  } else {
     const int l = nl - 1;
     Level& L = m->L[l];
     const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
@@ -601,7 +710,7 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
     }
   }
   // ---- ascent (multigrid.hpp:1843-2000)
-  for (int l = nl - 2; l >= 0; --l) {
+  for (int l = std::min(nl - 2, lc - 1); l >= 0; --l) {
     Level& L = m->L[l];
     const T* b = (l == 0) ? rhs_top : Prec<T>::rhs(L);
     T* cur = sol[l];
@@ -704,9 +813,6 @@ static int body(fb_mg* m) {
     FB_CHECK_LAUNCH();
     if (low) k_pcg_dir<float><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const float*)z, m->sc, n);
     else     k_pcg_dir<double><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const double*)z, m->sc, n);
-    m->launches++;
-    FB_CHECK_LAUNCH();
-    k_commit_gamma<<<1, 1, 0, m->stream>>>(m->sc);
     m->launches++;
     FB_CHECK_LAUNCH();
     EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
@@ -990,6 +1096,7 @@ int common_init(fb_mg* m) {
   FB_TRY(dalloc(m, &m->dbg_err, 1));
   FB_CUDA(cudaMemsetAsync(m->dbg_err, 0, sizeof(unsigned long long), m->stream));
   FB_TRY(dalloc(m, &m->kerr, 1));
+  FB_TRY(dalloc(m, &m->cred, 64));
   FB_CUDA(cudaMemsetAsync(m->kerr, 0, sizeof(unsigned), m->stream));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
