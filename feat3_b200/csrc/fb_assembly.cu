@@ -505,6 +505,7 @@ static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
   FB_TRY(dalloc(m, &L.mask, (n + 31) / 32));
   k_mask<<<grid_for((n + 31) / 32, 256), 256, 0, m->stream>>>(g, n, L.mask);
   FB_CHECK_LAUNCH();
+  L.mask_boundary = true;
   return FB_OK;
 }
 

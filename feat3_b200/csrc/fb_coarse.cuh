@@ -144,6 +144,26 @@ __device__ __forceinline__ T coarse_prol(const CLevel<T>& F, const CLevel<T>& C,
   return s;
 }
 
+// one Jacobi step at row i from the product s (EpiJacobi without skip)
+template<typename T>
+__device__ __forceinline__ T jacobi_row(const CLevel<T>& L, T om, const T* cur, const T* b, uint32_t i, T s) {
+  const T xc = ldc(cur + i);
+  const T d = ldc(b + i) - s;
+  return masked(L.mask, i) ? xc : om * (__ldg(L.invd + i) * d) + xc;
+}
+
+// post-smoothing step at row i (EpiJacobi with s0 and skip test; the first step reduces ||d||^2)
+template<typename T>
+__device__ __forceinline__ T post_row(const CLevel<T>& L, T om, const T* cur, const T* b, const T* s0, uint32_t i, T s,
+                                      bool skip, bool first, double& acc) {
+  if (skip) return ldc(s0 + i);
+  const T xc = ldc(cur + i);
+  const T d = ldc(b + i) - s;
+  if (masked(L.mask, i)) return xc;
+  if (first) acc += double(d) * double(d);
+  return om * (__ldg(L.invd + i) * d) + xc;
+}
+
 // deterministic cluster-wide sum; ends with a cluster barrier, result in every thread
 template<int THREADS>
 __device__ __forceinline__ double cluster_sum(double v, double* scratch, double* sh,
@@ -184,22 +204,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
     for (int it = 1; it < nu; ++it) {
       for (uint32_t i = gt; i < L.n; i += gs) {
         const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
-        T o;
-        if (skip) o = T(0);
-        else {
-          const T xc = ldc(cur + i);
-          const T d = ldc(b + i) - s;
-          o = masked(L.mask, i) ? xc : om * (__ldg(L.invd + i) * d) + xc;
-        }
-        oth[i] = o;
+        oth[i] = skip ? T(0) : jacobi_row(L, om, cur, b, i, s);
       }
       cl.sync();
       T* tmp = cur; cur = oth; oth = tmp;
     }
     sol[l] = cur;
     for (uint32_t i = gt; i < L.n; i += gs) {
-      const T d = ldc(b + i) - coarse_row<T, DIM>(L, cur, int32_t(i));
-      L.def[i] = masked(L.mask, i) ? T(0) : d;
+      const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
+      L.def[i] = masked(L.mask, i) ? T(0) : ldc(b + i) - s;
     }
     cl.sync();
     const CLevel<T>& C = A.L[l + 1];
@@ -280,18 +293,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
       const bool skip = it > 0 && (!isfinite(dv) || dv <= double(eps_of<T>()) * double(eps_of<T>()));
       for (uint32_t i = gt; i < L.n; i += gs) {
         const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
-        T o;
-        if (skip) o = ldc(s0 + i);
-        else {
-          const T xc = ldc(cur + i);
-          const T d = ldc(b + i) - s;
-          if (masked(L.mask, i)) o = xc;
-          else {
-            o = om * (__ldg(L.invd + i) * d) + xc;
-            if (it == 0) acc += double(d) * double(d);
-          }
-        }
-        oth[i] = o;
+        oth[i] = post_row(L, om, cur, b, s0, i, s, skip, it == 0, acc);
       }
       if (it == 0) {
         dn = cluster_sum<THREADS>(acc, A.red + 32 * (rk++ & 1), sh, cl);

@@ -207,6 +207,18 @@ __device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __res
   return s;
 }
 
+// sums of the cell coefficients of cell line c (kw[oz][c][ox]) over the cells that a
+// neighbour offset (dz, dx) in {-1,0,1}^2 selects: -1 -> the lower cell, +1 -> the upper one,
+// 0 -> both; K[dz+1][dx+1]
+template<typename T>
+__device__ __forceinline__ void ksums(const T (&kw)[2][2][2], int c, T (&K)[3][3]) {
+  const T k00 = kw[0][c][0], k01 = kw[0][c][1], k10 = kw[1][c][0], k11 = kw[1][c][1];
+  K[0][0] = k00; K[0][2] = k01; K[2][0] = k10; K[2][2] = k11;
+  K[0][1] = k00 + k01; K[2][1] = k10 + k11;
+  K[1][0] = k00 + k10; K[1][2] = k01 + k11;
+  K[1][1] = K[0][1] + K[2][1];
+}
+
 // ------------------------------------------------------------------ the tiled kernel
 // 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
 template<typename T, typename Epi, int NST, int MINB, int TY>
@@ -352,6 +364,9 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
           kw[q][0][0] = A.k ? ks[q][0] : T(1);
           kw[q][0][1] = A.k ? ks[q][1] : T(1);
         }
+        // per cell line: sums of k over the cells selected by (dz, dx) in {-1,0,1}^2
+        T K[2][3][3];
+        ksums(kw, 0, K[0]);
 #pragma unroll
         for (int j = 0; j < TY; ++j) {
           if (l0 + j >= g.lt) break;
@@ -364,17 +379,26 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
             kw[q][1][0] = A.k ? ks[q][(j + 1) * N] : T(1);
             kw[q][1][1] = A.k ? ks[q][(j + 1) * N + 1] : T(1);
           }
-          T s = T(0);
+          // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
+          // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
+          // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b])
+          ksums(kw, 1, K[1]);
+          T S[8];
 #pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int ox = e & 1, oy = (e >> 1) & 1, oz = (e >> 2) & 1;
-            const int a = (1 - ox) | ((1 - oy) << 1) | ((1 - oz) << 2);
-            T in = T(0);
+          for (int r = 0; r < 8; ++r) S[r] = T(0);
 #pragma unroll
-            for (int b = 0; b < 8; ++b)
-              in += A.kr[a ^ b] * xw[oz + ((b >> 2) & 1)][oy + ((b >> 1) & 1)][ox + (b & 1)];
-            s += kw[oz][oy][ox] * in;
-          }
+          for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+              for (int dx = 0; dx < 3; ++dx) {
+                const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
+                const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
+                S[r] += Kd * xw[dz][dy][dx];
+              }
+          T s = A.kr[0] * S[0];
+#pragma unroll
+          for (int r = 1; r < 8; ++r) s += A.kr[r] * S[r];
           const uint32_t row = r0 + (l0 + j) * M1 + X;
           T sv[NS > 0 ? NS : 1];
           if (NS > 0) sv[0] = ss[j * int(M1)];
@@ -394,6 +418,10 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
             kw[q][0][0] = kw[q][1][0];
             kw[q][0][1] = kw[q][1][1];
           }
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) K[0][a][b] = K[1][a][b];
         }
       }
       __syncwarp();

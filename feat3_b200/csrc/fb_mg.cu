@@ -390,7 +390,8 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
   constexpr int TY = sizeof(T) == 4 ? 4 : 2;
   const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
-  const uint32_t* mask = SE::mask(epi);
+  // a structured level's filter is its lattice boundary, which no tile row touches
+  const uint32_t* mask = (L.mask_boundary && SE::mask(epi) == L.mask) ? nullptr : SE::mask(epi);
   MfTile G;
   G.M1 = M1; G.N = N;
   G.G = std::max<uint32_t>(1, 256 / W);
@@ -550,7 +551,7 @@ static int presmooth(fb_mg* m, int l, const T* b, const double* bnorm, bool need
 
 // ------------------------------------------------------------------ fused coarse cycle
 constexpr uint32_t kCoarseRows = 40000;  // levels up to this size go to the one-cluster kernel
-constexpr int kCoarseThreads = 512;
+template<typename T> constexpr int coarse_threads() { return 512; }
 
 template<typename T, int DIM>
 static int coarse_cluster_size(fb_mg* m) {
@@ -558,7 +559,7 @@ static int coarse_cluster_size(fb_mg* m) {
   static int cs = -1;
   if (cs >= 0) return cs;
   cs = 0;
-  auto fn = k_coarse_cycle<T, DIM, kCoarseThreads>;
+  auto fn = k_coarse_cycle<T, DIM, coarse_threads<T>()>;
   (void)m;
   for (int want : {16, 8}) {
     if (want > 8 && cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
@@ -567,7 +568,7 @@ static int coarse_cluster_size(fb_mg* m) {
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(want);
-    cfg.blockDim = dim3(kCoarseThreads);
+    cfg.blockDim = dim3(coarse_threads<T>());
     cudaLaunchAttribute at;
     at.id = cudaLaunchAttributeClusterDimension;
     at.val.clusterDim.x = want; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
@@ -625,15 +626,15 @@ static int launch_coarse(fb_mg* m, int lc, T** sol_lc) {
   const int cs = m->dim == 3 ? coarse_cluster_size<T, 3>(m) : coarse_cluster_size<T, 2>(m);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs);
-  cfg.blockDim = dim3(kCoarseThreads);
+  cfg.blockDim = dim3(coarse_threads<T>());
   cfg.stream = m->stream;
   cudaLaunchAttribute at;
   at.id = cudaLaunchAttributeClusterDimension;
   at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
   cfg.attrs = &at;
   cfg.numAttrs = 1;
-  if (m->dim == 3) FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 3, kCoarseThreads>, A));
-  else FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 2, kCoarseThreads>, A));
+  if (m->dim == 3) FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 3, coarse_threads<T>()>, A));
+  else FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 2, coarse_threads<T>()>, A));
   m->launches++;
   FB_CHECK_LAUNCH();
   // the kernel's pointer walk: nu - 1 swaps in the pre-smoothing of level lc, nu in its post-smoothing

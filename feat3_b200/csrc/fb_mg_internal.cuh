@@ -69,6 +69,7 @@ struct Level {
   double* invd64 = nullptr;
   float* invd32 = nullptr;
   uint32_t* mask = nullptr;
+  bool mask_boundary = false;  // the mask is exactly the lattice boundary (structured levels)
   uint32_t* filt = nullptr;
   uint32_t nfilt = 0;
   double *rhs64 = nullptr, *x64 = nullptr, *y64 = nullptr, *def64 = nullptr;
