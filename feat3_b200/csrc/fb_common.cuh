@@ -104,8 +104,9 @@ __device__ __forceinline__ bool reduce_finish(double blk, double* ws, unsigned* 
   if (!am_last) return false;
   __threadfence();
   double v = 0.0;
-  // fixed order: thread t sums partials t, t+THREADS, ...
-  for (unsigned i = threadIdx.x; i < gridDim.x; i += THREADS) v += ((volatile double*)ws)[i];
+  // fixed order: thread t sums partials t, t+THREADS, ... (L2 loads, free to overlap)
+#pragma unroll 4
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += THREADS) v += __ldcg(ws + i);
   v = block_sum<THREADS>(v, sh);
   if (threadIdx.x == 0) {
     *out = take_sqrt ? sqrt(v) : v;
@@ -130,7 +131,8 @@ __device__ __forceinline__ bool reduce_finish_nd(double blk, double* ws, unsigne
   if (!am_last) return false;
   __threadfence();
   double v = 0.0;
-  for (uint32_t i = tid; i < nblk; i += THREADS) v += ((volatile double*)ws)[i];
+#pragma unroll 4
+  for (uint32_t i = tid; i < nblk; i += THREADS) v += __ldcg(ws + i);
   // block_sum indexes by threadIdx.x: flatten is equivalent for 1D-flattened warps
   v = warp_sum(v);
   const int lane = tid & 31, wid = tid >> 5;

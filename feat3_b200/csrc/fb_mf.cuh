@@ -11,7 +11,8 @@
 // line column with a sliding window (9 new x values and 4 new cell coefficients per row,
 // the other 18 + 4 are kept in registers). Rows outside
 // the tiles (the lattice boundary planes and lines and the two ends of interior lines) are
-// formed afterwards by the same warps with direct loads.
+// formed by the same warps with direct loads before they take their first tile, while the
+// producer's first copies are in flight.
 //
 // Every wait on an mbarrier is bounded (about one second of %globaltimer); on expiry the
 // kernel records the event in `kerr`, stops taking tiles, waits (bounded) for its copies in
@@ -26,9 +27,9 @@ namespace fb {
 // receives the product s, the row's own x value xc and the staged stream values st[].
 template<typename Epi> struct Staged { static constexpr bool kOk = false; static constexpr int kStreams = 0; };
 
-template<typename T, bool RED>
-struct Staged<EpiJacobi<T, RED>> {
-  using E = EpiJacobi<T, RED>;
+template<typename T, bool RED, bool DOT>
+struct Staged<EpiJacobi<T, RED, DOT>> {
+  using E = EpiJacobi<T, RED, DOT>;
   static constexpr bool kOk = true;
   static constexpr int kStreams = 2;
   static const void* stream(const E& e, int i) { return i == 0 ? (const void*)e.rhs : (const void*)e.invd; }
@@ -37,17 +38,19 @@ struct Staged<EpiJacobi<T, RED>> {
   __device__ static bool skip(const E& e) { return smoother_skip<T>(e.skip_src); }
   __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st, bool m) {
     if (skp) {
-      e.out[row] = e.s0 ? e.s0[row] : T(0);
-      return 0.0;
+      const T o = e.s0 ? e.s0[row] : T(0);
+      e.out[row] = o;
+      return DOT ? double(o) * double(st[0]) : 0.0;
     }
     const T d = st[0] - s;
     if (m) {
       e.out[row] = xc;
-      return 0.0;
+      return DOT ? double(xc) * double(st[0]) : 0.0;
     }
     const T t = st[1] * d;
-    e.out[row] = e.omega * t + xc;
-    return RED ? double(d) * double(d) : 0.0;
+    const T o = e.omega * t + xc;
+    e.out[row] = o;
+    return RED ? double(d) * double(d) : (DOT ? double(o) * double(st[0]) : 0.0);
   }
 };
 
@@ -310,6 +313,32 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
     }
     __syncwarp();
   } else {
+    // ---------------- direct path first: boundary lines and the end points of interior lines
+    // (rows no tile holds; done while the producer fills the first stages)
+    {
+      const uint32_t cpl = (M1 + 31) / 32;  // chunks per boundary line
+      const uint32_t nitems = G.nbl_items + G.nedge_items;
+      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
+        int32_t row = -1;
+        if (item < G.nbl_items) {
+          const uint32_t bl = item / cpl, X = (item % cpl) * 32 + lane;
+          uint32_t Y, Z;
+          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl % M1; }
+          else { const uint32_t r = bl - 2 * M1; Z = 1 + r / 2; Y = (r & 1) ? M1 - 1 : 0; }
+          if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
+        } else {
+          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
+          if (li < W * W) {
+            const uint32_t Y = 1 + li % W, Z = 1 + li / W;
+            row = int32_t((Z * M1 + Y) * M1 + ((lane & 1) ? M1 - 1 : 0));
+          }
+        }
+        if (row >= 0) {
+          const T s = mf_row_direct<T>(A, x, row);
+          acc += epi(uint32_t(row), s);
+        }
+      }
+    }
     // ---------------- consumers: TY rows per thread and tile (sliding window along Y)
     const bool skp = SE::skip(epi);
     const uint32_t tid = threadIdx.x;
@@ -426,31 +455,6 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
-    }
-    // ---------------- direct path: boundary lines and the end points of interior lines
-    if (ok) {
-      const uint32_t cpl = (M1 + 31) / 32;  // chunks per boundary line
-      const uint32_t nitems = G.nbl_items + G.nedge_items;
-      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
-        int32_t row = -1;
-        if (item < G.nbl_items) {
-          const uint32_t bl = item / cpl, X = (item % cpl) * 32 + lane;
-          uint32_t Y, Z;
-          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl % M1; }
-          else { const uint32_t r = bl - 2 * M1; Z = 1 + r / 2; Y = (r & 1) ? M1 - 1 : 0; }
-          if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
-        } else {
-          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
-          if (li < W * W) {
-            const uint32_t Y = 1 + li % W, Z = 1 + li / W;
-            row = int32_t((Z * M1 + Y) * M1 + ((lane & 1) ? M1 - 1 : 0));
-          }
-        }
-        if (row >= 0) {
-          const T s = mf_row_direct<T>(A, x, row);
-          acc += epi(uint32_t(row), s);
-        }
-      }
     }
   }
   if (Epi::kReduce) {

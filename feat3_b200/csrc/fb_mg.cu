@@ -484,9 +484,9 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
   if (use_q1_transfer(m, L)) {
     if constexpr (std::is_same<Epi, EpiRestrict<T>>::value) {
       if (L.tr.dim == 3) {
-        constexpr int ZB = 2;
-        const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, (L.tr.Mc1 + ZB - 1) / ZB);
-        k_rest_q1_3d<T, ZB><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
+        constexpr int CZ = sizeof(T) == 4 ? 4 : 2;  // static shared tile below 48 KB
+        const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, (L.tr.Mc1 + CZ - 1) / CZ);
+        k_rest_q1_tile<T, CZ><<<grid, 256, 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
@@ -509,9 +509,9 @@ static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
   if (use_q1_transfer(m, L)) {
     if constexpr (std::is_same<Epi, EpiProlong<T>>::value) {
       if (L.tr.dim == 3) {
-        constexpr int ZB = 8;
-        const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + ZB - 1) / ZB);
-        k_prol_q1_3d<T, ZB><<<grid, dim3(32, 8), 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask);
+        const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + 7) / 8);
+        const int bmask = L.mask_boundary && epi.mask == L.mask;
+        k_prol_q1_tile<T><<<grid, 256, 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask, bmask);
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
@@ -729,6 +729,10 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
           m->launches++;
           FB_CHECK_LAUNCH();
         }
+      } else if (l == 0 && it == nu - 1 && m->top_dot) {
+        // the result is z: form PCG's r . z (rhs = r, or its FP32 copy in the mixed form) here
+        EpiJacobi<T, false, true> e{cur, b, Prec<T>::invd(L), oth, s0, L.mask, dn, omega};
+        FB_TRY(spmv_L<T>(m, L, cur, e, &m->sc->rz));
       } else {
         EpiJacobi<T, false> e{cur, b, Prec<T>::invd(L), oth, s0, L.mask, dn, omega};
         FB_TRY(spmv_L<T>(m, L, cur, e, nullptr));
@@ -771,6 +775,11 @@ struct Stop {
 static bool fuse_s1(const fb_mg* m) {
   return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1;
 }
+// ... and its last post-smoothing step forms r . z (z = that step's result, r = the V-cycle's
+// right-hand side: the outer defect, or its FP32 copy in the mixed forms)
+static bool fuse_dot(const fb_mg* m) {
+  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1 && m->dot_fuse;
+}
 
 // outer defect r = filter_def(b - A x), ||r||^2, FP32 copy for the mixed V-cycle
 static int outer_defect(fb_mg* m) {
@@ -803,15 +812,20 @@ static int body(fb_mg* m) {
   const bool low = m->cfg.precision != FB_PREC_F64;
   const void* z = nullptr;
   m->top_s1 = fuse_s1(m);
+  m->top_dot = fuse_dot(m);
   const int pst = precond(m, &z);
   m->top_s1 = false;
+  const bool dot_done = m->top_dot;
+  m->top_dot = false;
   FB_TRY(pst);
   if (m->cfg.outer == FB_OUTER_PCG) {
     // gamma' = r . z ; p = z + beta p ; q = A p ; x, r update
-    if (low) k_dot_rz<float><<<occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz);
-    else     k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const double*)z, n, m->ws, m->counter, &m->sc->rz);
-    m->launches++;
-    FB_CHECK_LAUNCH();
+    if (!dot_done) {
+      if (low) k_dot_rz<float><<<occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz);
+      else     k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const double*)z, n, m->ws, m->counter, &m->sc->rz);
+      m->launches++;
+      FB_CHECK_LAUNCH();
+    }
     if (low) k_pcg_dir<float><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const float*)z, m->sc, n);
     else     k_pcg_dir<double><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const double*)z, m->sc, n);
     m->launches++;

@@ -126,6 +126,8 @@ struct fb_mg {
   int launches = 0;
   int body_launches = 0;
   bool top_s1 = false;
+  bool top_dot = false;                  // the V-cycle's last finest-level step also forms r . z
+  bool dot_fuse = true;
   unsigned long long* dbg_err = nullptr;  // FB_DEBUG=1: device word for kernel self-checks
   unsigned* kerr = nullptr;               // set by a staged kernel whose bounded wait expired
   double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)

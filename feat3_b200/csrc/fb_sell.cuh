@@ -80,25 +80,30 @@ struct EpiDefect {
 
 // one damped-Jacobi Richardson step on the level system (fused defect + update):
 //   out = x + omega * filter_cor(invd o (rhs - A x)); skip => out = s0 (0 if s0 == nullptr)
-// reduction: ||filter_def(rhs - A x)||^2 (initial defect of the smoother, post-smoothing)
-template<typename T, bool RED>
+// reduction: RED: ||filter_def(rhs - A x)||^2 (initial defect of the smoother, post-smoothing);
+// DOT: out . rhs (the last post-smoothing step of the finest level, whose result is the
+// preconditioned defect z and whose rhs is the outer defect r: PCG's r . z)
+template<typename T, bool RED, bool DOT = false>
 struct EpiJacobi {
-  static constexpr bool kReduce = RED;
+  static constexpr bool kReduce = RED || DOT;
   const T* x; const T* rhs; const T* invd; T* out; const T* s0; const uint32_t* mask;
   const double* skip_src; T omega;
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
     if (smoother_skip<T>(skip_src)) {
-      out[row] = s0 ? s0[row] : T(0);
-      return 0.0;
+      const T o = s0 ? s0[row] : T(0);
+      out[row] = o;
+      return DOT ? double(o) * double(rhs[row]) : 0.0;
     }
     const T d = rhs[row] - s;
     if (masked(mask, row)) {
-      out[row] = x[row];
-      return 0.0;
+      const T o = x[row];
+      out[row] = o;
+      return DOT ? double(o) * double(rhs[row]) : 0.0;
     }
     const T t = invd[row] * d;
-    out[row] = omega * t + x[row];
-    return RED ? double(d) * double(d) : 0.0;
+    const T o = omega * t + x[row];
+    out[row] = o;
+    return RED ? double(d) * double(d) : (DOT ? double(o) * double(rhs[row]) : 0.0);
   }
 };
 
@@ -686,6 +691,148 @@ __global__ void __launch_bounds__(256) k_rest_q1_3d(Q1Transfer g, const T* __res
   const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
   const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
+}
+
+// 3D restriction with the fine block staged in shared memory: a block owns 32 x 8 x CZ coarse
+// points and first loads the (65 x 17 x (2 CZ + 1)) fine values around them with coalesced
+// loads (indices clamped; a clamped value always meets weight 0), then every thread forms CZ
+// coarse rows from shared memory. Terms and their order are those of k_rest_q1.
+// Launched on a (ceil(Mc1/32), ceil(Mc1/8), ceil(Mc1/CZ)) grid of 256 threads.
+template<typename T, int CZ>
+__global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __restrict__ xf, EpiRestrict<T> epi,
+                                                      double* ws, unsigned* counter, double* red_out) {
+  constexpr int SX = 65, SY = 17, SZ = 2 * CZ + 1;
+  __shared__ T sm[SZ][SY][SX];
+  __shared__ double sh[8];
+  const int X0 = int(blockIdx.x) * 32, Y0 = int(blockIdx.y) * 8, Z0 = int(blockIdx.z) * CZ;
+  const int F = int(g.Mf1) - 1;
+  const int fx0 = 2 * X0 - 1, fy0 = 2 * Y0 - 1, fz0 = 2 * Z0 - 1;
+  // one warp per fine line segment of 65 values (no index division)
+  const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
+#pragma unroll 4
+  for (int r = wrp; r < SY * SZ; r += 8) {
+    const int ly = r % SY, lz = r / SY;
+    int fy = fy0 + ly, fz = fz0 + lz;
+    fy = fy < 0 ? 0 : (fy > F ? F : fy);
+    fz = fz < 0 ? 0 : (fz > F ? F : fz);
+    const T* line = xf + (size_t(fz) * g.Mf1 + fy) * g.Mf1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int lx = lane + 32 * k;
+      if (lx < SX) {
+        int fx = fx0 + lx;
+        fx = fx < 0 ? 0 : (fx > F ? F : fx);
+        sm[lz][ly][lx] = line[fx];
+      }
+    }
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int X = X0 + tx, Y = Y0 + ty;
+  double acc = 0.0;
+  if (X < int(g.Mc1) && Y < int(g.Mc1)) {
+    T wx[3], wy[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int ox = 2 * X + d - 1, oy = 2 * Y + d - 1;
+      const T wd = d == 1 ? T(1) : T(0.5);
+      wx[d] = (ox < 0 || ox > F) ? T(0) : wd;
+      wy[d] = (oy < 0 || oy > F) ? T(0) : wd;
+    }
+#pragma unroll
+    for (int cz = 0; cz < CZ; ++cz) {
+      const int Z = Z0 + cz;
+      if (Z >= int(g.Mc1)) break;
+      T wz[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const int oz = 2 * Z + d - 1;
+        wz[d] = (oz < 0 || oz > F) ? T(0) : (d == 1 ? T(1) : T(0.5));
+      }
+      T s = T(0);
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s += (wx[c] * wy[b] * wz[a]) * sm[2 * cz + a][2 * ty + b][2 * tx + c];
+      const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
+      acc += epi(i, s);
+    }
+  }
+  const double blk = block_sum<256>(acc, sh);
+  const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
+  const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
+}
+
+// 3D prolongation + coarse-grid correction with the coarse block in shared memory: a block
+// owns 32 x 8 x 8 fine points; it loads the 17 x 5 x 5 coarse values behind them, then every
+// thread loads the 8 iterate values of its fine column at once and forms the 8 corrections.
+// `bmask` (structured levels): the filter is the lattice boundary, evaluated from coordinates
+// instead of read. Terms and their order are those of k_prol_q1.
+// Launched on a (ceil(Mf1/32), ceil(Mf1/8), ceil(Mf1/8)) grid of 256 threads.
+template<typename T>
+__global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __restrict__ xc, T* __restrict__ sol,
+                                                      const uint32_t* __restrict__ mask, int bmask) {
+  constexpr int CX = 17, CY = 5, CZ = 5;
+  __shared__ T cm[CZ][CY][CX];
+  const uint32_t X0 = blockIdx.x * 32, Y0 = blockIdx.y * 8, Z0 = blockIdx.z * 8;
+  const uint32_t cx0 = X0 >> 1, cy0 = Y0 >> 1, cz0 = Z0 >> 1;
+  const uint32_t Cm = g.Mc1 - 1;
+  // this thread's iterate column first: its loads are in flight while the coarse block arrives
+  const uint32_t tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const uint32_t X = X0 + tx, Y = Y0 + ty;
+  const bool act = X < g.Mf1 && Y < g.Mf1;
+  const size_t plane = size_t(g.Mf1) * g.Mf1;
+  const size_t i0 = act ? X + size_t(g.Mf1) * (Y + size_t(g.Mf1) * Z0) : 0;
+  T old[8];
+#pragma unroll
+  for (int z = 0; z < 8; ++z) old[z] = (act && Z0 + z < g.Mf1) ? sol[i0 + z * plane] : T(0);
+  {
+    // one warp per coarse line segment of 17 values
+    const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
+    for (int r = wrp; r < CY * CZ; r += 8) {
+      const int ly = r % CY, lz = r / CY;
+      if (lane < CX) {
+        const uint32_t cx = min(cx0 + lane, Cm), cy = min(cy0 + ly, Cm), cz = min(cz0 + lz, Cm);
+        cm[lz][ly][lane] = xc[(size_t(cz) * g.Mc1 + cy) * g.Mc1 + cx];
+      }
+    }
+  }
+  __syncthreads();
+  if (!act) return;
+  bool msk[8];
+  const bool bxy = X == 0 || X == g.Mf1 - 1 || Y == 0 || Y == g.Mf1 - 1;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    const bool in = Z0 + z < g.Mf1;
+    const size_t i = in ? i0 + z * plane : i0;
+    if (bmask) msk[z] = bxy || Z0 + z == 0 || Z0 + z == g.Mf1 - 1;
+    else msk[z] = mask ? ((__ldg(mask + (i >> 5)) >> (i & 31)) & 1u) : false;
+  }
+  const uint32_t lx0 = (X >> 1) - cx0, lx1 = ((X + 1) >> 1) - cx0;
+  const uint32_t ly0 = (Y >> 1) - cy0, ly1 = ((Y + 1) >> 1) - cy0;
+  const T hx = (X & 1) ? T(0.5) : T(1), hy = (Y & 1) ? T(0.5) : T(1);
+  const T wy1 = (Y & 1) ? T(1) : T(0);
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    if (Z0 + z >= g.Mf1) break;
+    const T w = hx * hy * ((z & 1) ? T(0.5) : T(1));
+    const T wx1 = (X & 1) ? w : T(0);
+    const T wz1 = (z & 1) ? T(1) : T(0);
+    const int q0 = z >> 1, q1 = (z + 1) >> 1;
+    T s = T(0);
+    s += w * cm[q0][ly0][lx0];
+    s += wx1 * cm[q0][ly0][lx1];
+    s += (wy1 * w) * cm[q0][ly1][lx0];
+    s += (wy1 * wx1) * cm[q0][ly1][lx1];
+    s += (wz1 * w) * cm[q1][ly0][lx0];
+    s += (wz1 * wx1) * cm[q1][ly0][lx1];
+    s += (wz1 * wy1 * w) * cm[q1][ly1][lx0];
+    s += (wz1 * wy1 * wx1) * cm[q1][ly1][lx1];
+    if (!msk[z]) sol[i0 + z * plane] = T(1) * s + old[z];
+  }
 }
 
 }  // namespace fb
