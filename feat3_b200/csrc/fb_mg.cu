@@ -442,7 +442,7 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   }
   for (int j = 0; j < (DIM == 3 ? 27 : 9); ++j) v.off[j] = L.St.off[j];
   if constexpr (DIM == 3 && Staged<Epi>::kOk) {
-    if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err)
+    if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err && !(m->cfg.flags & FB_FLAG_NO_TILED))
       return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
   }
   auto fn = k_mf_q1<T, Epi, DIM>;
@@ -585,7 +585,8 @@ static int coarse_cluster_size(fb_mg* m) {
 template<typename T>
 static int coarse_start(fb_mg* m) {
   const int nl = (int)m->L.size();
-  if (m->cfg.format != FB_FORMAT_MATFREE || m->cfg.coarse == FB_COARSE_PCG || !m->coarse_fuse) return nl;
+  if (m->cfg.format != FB_FORMAT_MATFREE || m->cfg.coarse == FB_COARSE_PCG || (m->cfg.flags & FB_FLAG_NO_COARSE_FUSION))
+    return nl;
   int lc = nl;
   for (int l = nl - 1; l >= 1; --l) {
     if (!m->L[l].mf || m->L[l].n > kCoarseRows) break;
@@ -778,7 +779,7 @@ static bool fuse_s1(const fb_mg* m) {
 // ... and its last post-smoothing step forms r . z (z = that step's result, r = the V-cycle's
 // right-hand side: the outer defect, or its FP32 copy in the mixed forms)
 static bool fuse_dot(const fb_mg* m) {
-  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1 && m->dot_fuse;
+  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1 && !(m->cfg.flags & FB_FLAG_NO_DOT_FUSION);
 }
 
 // outer defect r = filter_def(b - A x), ||r||^2, FP32 copy for the mixed V-cycle
@@ -855,7 +856,7 @@ static int body(fb_mg* m) {
 
 static int run_body(fb_mg* m) {
   if (!m->cfg.use_graphs || debug_enabled()) return body(m);
-  const int key = m->cfg.format * 64 + m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
+  const int key = m->cfg.flags * 256 + m->cfg.format * 64 + m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
   if (!m->g_body || m->g_body_key != key) {
     if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; }
     cudaGraph_t g = nullptr;
@@ -1240,6 +1241,7 @@ void fb_solver_cfg_default(fb_solver_cfg* c) {
   c->precision = FB_PREC_F64;
   c->use_graphs = 1;
   c->format = FB_FORMAT_SELL;
+  c->flags = 0;
 }
 
 int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {

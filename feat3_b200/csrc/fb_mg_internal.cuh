@@ -127,11 +127,9 @@ struct fb_mg {
   int body_launches = 0;
   bool top_s1 = false;
   bool top_dot = false;                  // the V-cycle's last finest-level step also forms r . z
-  bool dot_fuse = true;
   unsigned long long* dbg_err = nullptr;  // FB_DEBUG=1: device word for kernel self-checks
   unsigned* kerr = nullptr;               // set by a staged kernel whose bounded wait expired
-  double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)
-  bool coarse_fuse = true;                // run the coarse end of the V-cycle as one cluster launch                   // finest-level first smoothing step already formed (fused)
+  double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)                   // finest-level first smoothing step already formed (fused)
   double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
   double* adj = nullptr;                 // adjoint right-hand side
 };

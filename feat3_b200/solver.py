@@ -103,9 +103,13 @@ class MultiGrid:
 
     # ---------------------------------------------------------------- configuration
     def configure(self, outer="pcg", nu=4, omega_jac=0.5, omega_rich=1.0, omega_outer=1.0, coarse="direct",
-                  tol=1e-8, max_iter=1000, precision="f64", graphs=True, format="sell"):
+                  tol=1e-8, max_iter=1000, precision="f64", graphs=True, format="sell", fuse_coarse=True,
+                  fuse_dot=True, tiled=True):
+        """Solver configuration (fb_solver_cfg). fuse_coarse / fuse_dot / tiled switch individual
+        fusions of the matrix-free form off (FB_FLAG_*), for comparisons; the results agree."""
+        flags = (0 if fuse_coarse else 1) | (0 if fuse_dot else 2) | (0 if tiled else 4)
         cfg = _lib.SolverCfg(OUTER[outer], nu, omega_jac, omega_rich, omega_outer, COARSE[coarse], tol, max_iter,
-                             PRECISION[precision], 1 if graphs else 0, FORMAT[format])
+                             PRECISION[precision], 1 if graphs else 0, FORMAT[format], flags)
         _lib.check("fb_mg_configure", _lib.load().fb_mg_configure(self.h, C.byref(cfg)))
         self.cfg = cfg
         return self

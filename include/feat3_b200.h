@@ -218,7 +218,14 @@ typedef struct fb_solver_cfg {
   int precision;
   int use_graphs;     /* capture the per-iteration launch sequence in a CUDA graph */
   int format;         /* FB_FORMAT_SELL, FB_FORMAT_STENCIL or FB_FORMAT_MATFREE */
+  int flags;          /* FB_FLAG_*: switch individual fusions off (testing; 0 = all on) */
 } fb_solver_cfg;
+/* flags: the coarse end of the V-cycle level by level instead of one cluster launch; PCG's
+ * r . z as its own reduction instead of inside the last smoothing step; the matrix-free
+ * operator without the shared-memory tiled kernel */
+#define FB_FLAG_NO_COARSE_FUSION 1
+#define FB_FLAG_NO_DOT_FUSION 2
+#define FB_FLAG_NO_TILED 4
 FB_API void fb_solver_cfg_default(fb_solver_cfg* cfg);
 FB_API int fb_mg_configure(fb_mg* mg, const fb_solver_cfg* cfg);
 
