@@ -91,6 +91,7 @@ _SIGS = {
     "fb_mg_configure": [vp, C.POINTER(SolverCfg)],
     "fb_mg_solve": [vp, vp, vp, vp, C.POINTER(SolveInfo)],
     "fb_mg_solve_host": [vp, vp, vp, vp, C.POINTER(SolveInfo)],
+    "fb_mg_solve_host_zero": [vp, vp, vp, vp, C.POINTER(SolveInfo)],
     "fb_mg_vcycle": [vp, vp, vp],
     "fb_mg_assemble_rhs": [vp, i32, vp],
     "fb_mg_num_dofs": [vp, i32],

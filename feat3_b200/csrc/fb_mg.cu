@@ -387,7 +387,7 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
   constexpr int NS = SE::kStreams;
   constexpr int NST = 2;
   constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
-  constexpr int TY = sizeof(T) == 4 ? 4 : 2;
+  constexpr int TY = sizeof(T) == 4 ? 4 : 3;
   const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
   // a structured level's filter is its lattice boundary, which no tile row touches
@@ -509,9 +509,10 @@ static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
   if (use_q1_transfer(m, L)) {
     if constexpr (std::is_same<Epi, EpiProlong<T>>::value) {
       if (L.tr.dim == 3) {
-        const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + 7) / 8);
+        constexpr int FZ = 16;
+        const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + FZ - 1) / FZ);
         const int bmask = L.mask_boundary && epi.mask == L.mask;
-        k_prol_q1_tile<T><<<grid, 256, 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask, bmask);
+        k_prol_q1_tile<T, FZ><<<grid, 256, 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask, bmask);
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
@@ -1325,7 +1326,7 @@ int fb_mg_solve(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve
   return solve_dev(m, rhs, sol, hist, info);
 }
 
-int fb_mg_solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist, fb_solve_info* info) {
+static int solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist, fb_solve_info* info, bool zero) {
   if (!m || !rhs_h || !sol_h) return FB_ERR_INVALID;
   if (!m->configured) return FB_ERR_NOT_READY;
   FB_CUDA(cudaSetDevice(m->device));
@@ -1337,7 +1338,8 @@ int fb_mg_solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist,
   FB_CUDA(cudaEventCreate(&e1));
   FB_CUDA(cudaEventRecord(e0, m->stream));
   FB_CUDA(cudaMemcpyAsync(m->hb, rhs_h, sizeof(double) * n, cudaMemcpyHostToDevice, m->stream));
-  FB_CUDA(cudaMemcpyAsync(m->hx, sol_h, sizeof(double) * n, cudaMemcpyHostToDevice, m->stream));
+  if (zero) FB_CUDA(cudaMemsetAsync(m->hx, 0, sizeof(double) * n, m->stream));
+  else FB_CUDA(cudaMemcpyAsync(m->hx, sol_h, sizeof(double) * n, cudaMemcpyHostToDevice, m->stream));
   int st = solve_dev(m, m->hb, m->hx, hist, info);
   if (st == FB_OK) {
     if (cudaMemcpyAsync(sol_h, m->hx, sizeof(double) * n, cudaMemcpyDeviceToHost, m->stream) != cudaSuccess ||
@@ -1351,6 +1353,14 @@ int fb_mg_solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return st;
+}
+
+int fb_mg_solve_host(fb_mg* m, const double* rhs_h, double* sol_h, double* hist, fb_solve_info* info) {
+  return solve_host(m, rhs_h, sol_h, hist, info, false);
+}
+
+int fb_mg_solve_host_zero(fb_mg* m, const double* rhs_h, double* sol_h, double* hist, fb_solve_info* info) {
+  return solve_host(m, rhs_h, sol_h, hist, info, true);
 }
 
 int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {

@@ -739,6 +739,11 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
       wx[d] = (ox < 0 || ox > F) ? T(0) : wd;
       wy[d] = (oy < 0 || oy > F) ? T(0) : wd;
     }
+    T wxy[3][3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) wxy[b][c] = wx[c] * wy[b];
 #pragma unroll
     for (int cz = 0; cz < CZ; ++cz) {
       const int Z = Z0 + cz;
@@ -749,13 +754,14 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
         const int oz = 2 * Z + d - 1;
         wz[d] = (oz < 0 || oz > F) ? T(0) : (d == 1 ? T(1) : T(0.5));
       }
+      // the weights are powers of two: wxy * wz equals wx * wy * wz exactly
       T s = T(0);
 #pragma unroll
       for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) s += (wx[c] * wy[b] * wz[a]) * sm[2 * cz + a][2 * ty + b][2 * tx + c];
+          for (int c = 0; c < 3; ++c) s += (wxy[b][c] * wz[a]) * sm[2 * cz + a][2 * ty + b][2 * tx + c];
       const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
       acc += epi(i, s);
     }
@@ -767,17 +773,18 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
 }
 
 // 3D prolongation + coarse-grid correction with the coarse block in shared memory: a block
-// owns 32 x 8 x 8 fine points; it loads the 17 x 5 x 5 coarse values behind them, then every
-// thread loads the 8 iterate values of its fine column at once and forms the 8 corrections.
-// `bmask` (structured levels): the filter is the lattice boundary, evaluated from coordinates
-// instead of read. Terms and their order are those of k_prol_q1.
-// Launched on a (ceil(Mf1/32), ceil(Mf1/8), ceil(Mf1/8)) grid of 256 threads.
-template<typename T>
+// owns 32 x 8 x FZ fine points; every thread first loads the FZ iterate values of its fine
+// column (in flight together), the block loads the 17 x 5 x (FZ/2+1) coarse values behind the
+// tile, then every thread forms its FZ corrections. `bmask` (structured levels): the filter is
+// the lattice boundary, evaluated from coordinates instead of read. Terms and their order are
+// those of k_prol_q1. Launched on a (ceil(Mf1/32), ceil(Mf1/8), ceil(Mf1/FZ)) grid of 256 threads.
+template<typename T, int FZ>
 __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __restrict__ xc, T* __restrict__ sol,
                                                       const uint32_t* __restrict__ mask, int bmask) {
-  constexpr int CX = 17, CY = 5, CZ = 5;
+  static_assert(FZ % 2 == 0, "slabs start on even planes");
+  constexpr int CX = 17, CY = 5, CZ = FZ / 2 + 1;
   __shared__ T cm[CZ][CY][CX];
-  const uint32_t X0 = blockIdx.x * 32, Y0 = blockIdx.y * 8, Z0 = blockIdx.z * 8;
+  const uint32_t X0 = blockIdx.x * 32, Y0 = blockIdx.y * 8, Z0 = blockIdx.z * FZ;
   const uint32_t cx0 = X0 >> 1, cy0 = Y0 >> 1, cz0 = Z0 >> 1;
   const uint32_t Cm = g.Mc1 - 1;
   // this thread's iterate column first: its loads are in flight while the coarse block arrives
@@ -786,9 +793,9 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
   const bool act = X < g.Mf1 && Y < g.Mf1;
   const size_t plane = size_t(g.Mf1) * g.Mf1;
   const size_t i0 = act ? X + size_t(g.Mf1) * (Y + size_t(g.Mf1) * Z0) : 0;
-  T old[8];
+  T old[FZ];
 #pragma unroll
-  for (int z = 0; z < 8; ++z) old[z] = (act && Z0 + z < g.Mf1) ? sol[i0 + z * plane] : T(0);
+  for (int z = 0; z < FZ; ++z) old[z] = (act && Z0 + z < g.Mf1) ? sol[i0 + z * plane] : T(0);
   {
     // one warp per coarse line segment of 17 values
     const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
@@ -802,22 +809,18 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
   }
   __syncthreads();
   if (!act) return;
-  bool msk[8];
   const bool bxy = X == 0 || X == g.Mf1 - 1 || Y == 0 || Y == g.Mf1 - 1;
-#pragma unroll
-  for (int z = 0; z < 8; ++z) {
-    const bool in = Z0 + z < g.Mf1;
-    const size_t i = in ? i0 + z * plane : i0;
-    if (bmask) msk[z] = bxy || Z0 + z == 0 || Z0 + z == g.Mf1 - 1;
-    else msk[z] = mask ? ((__ldg(mask + (i >> 5)) >> (i & 31)) & 1u) : false;
-  }
   const uint32_t lx0 = (X >> 1) - cx0, lx1 = ((X + 1) >> 1) - cx0;
   const uint32_t ly0 = (Y >> 1) - cy0, ly1 = ((Y + 1) >> 1) - cy0;
   const T hx = (X & 1) ? T(0.5) : T(1), hy = (Y & 1) ? T(0.5) : T(1);
   const T wy1 = (Y & 1) ? T(1) : T(0);
 #pragma unroll
-  for (int z = 0; z < 8; ++z) {
+  for (int z = 0; z < FZ; ++z) {
     if (Z0 + z >= g.Mf1) break;
+    const size_t i = i0 + z * plane;
+    bool msk;
+    if (bmask) msk = bxy || Z0 + z == 0 || Z0 + z == g.Mf1 - 1;
+    else msk = mask ? ((__ldg(mask + (i >> 5)) >> (i & 31)) & 1u) : false;
     const T w = hx * hy * ((z & 1) ? T(0.5) : T(1));
     const T wx1 = (X & 1) ? w : T(0);
     const T wz1 = (z & 1) ? T(1) : T(0);
@@ -831,7 +834,7 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
     s += (wz1 * wx1) * cm[q1][ly0][lx1];
     s += (wz1 * wy1 * w) * cm[q1][ly1][lx0];
     s += (wz1 * wy1 * wx1) * cm[q1][ly1][lx1];
-    if (!msk[z]) sol[i0 + z * plane] = T(1) * s + old[z];
+    if (!msk) sol[i] = T(1) * s + old[z];
   }
 }
 

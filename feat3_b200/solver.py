@@ -160,16 +160,18 @@ class MultiGrid:
         out["u"] = sol
         return out
 
-    def solve_host(self, rhs, sol=None, record=True):
-        """End-to-end: host buffers in, host solution out (copies inside the timed region)."""
+    def solve_host(self, rhs, sol=None, record=True, zero_init=False):
+        """End-to-end: host buffers in, host solution out (copies inside the timed region).
+        zero_init: solve from a zero initial guess; sol is then output only and is not copied
+        to the device (fb_mg_solve_host_zero)."""
         if self.cfg is None:
             self.configure()
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         sol = np.zeros_like(rhs) if sol is None else np.ascontiguousarray(sol, dtype=np.float64)
         hist = np.zeros(self.cfg.max_iter + 1) if record else None
         info = _lib.SolveInfo()
-        _lib.call("fb_mg_solve_host", self.h, rhs.ctypes.data, sol.ctypes.data,
-                  None if hist is None else hist.ctypes.data, C.byref(info))
+        _lib.call("fb_mg_solve_host_zero" if zero_init else "fb_mg_solve_host", self.h, rhs.ctypes.data,
+                  sol.ctypes.data, None if hist is None else hist.ctypes.data, C.byref(info))
         out = self._info(info, hist)
         out["u"] = sol
         return out

@@ -247,6 +247,9 @@ typedef struct fb_solve_info {
 FB_API int fb_mg_solve(fb_mg* mg, const double* rhs, double* sol, double* hist, fb_solve_info* info);
 /* same with HOST buffers: uploads rhs and sol, solves, downloads sol (end-to-end path) */
 FB_API int fb_mg_solve_host(fb_mg* mg, const double* rhs_host, double* sol_host, double* hist, fb_solve_info* info);
+/* The same from a zero initial guess (sol_host is output only, so it is not copied to the device;
+ * Solver::solve after vec_sol.format()). */
+FB_API int fb_mg_solve_host_zero(fb_mg* mg, const double* rhs_host, double* sol_host, double* hist, fb_solve_info* info);
 /* one preconditioner application cor = MG(def) on the finest level (device pointers) */
 FB_API int fb_mg_vcycle(fb_mg* mg, const double* def, double* cor);
 

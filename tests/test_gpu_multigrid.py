@@ -133,6 +133,11 @@ def test_host_buffer_solve_matches_device_solve():
     r2 = mg.solve_host(b.cpu().numpy())
     assert r1["iters"] == r2["iters"]
     np.testing.assert_array_equal(r1["u"].cpu().numpy(), r2["u"])
+    # zero initial guess: whatever the output buffer holds is ignored
+    junk = np.full(b.numel(), np.nan)
+    r3 = mg.solve_host(b.cpu().numpy(), junk, zero_init=True)
+    assert r3["iters"] == r1["iters"]
+    np.testing.assert_array_equal(r1["u"].cpu().numpy(), r3["u"])
 
 
 def test_zero_rhs_and_nan_status():
