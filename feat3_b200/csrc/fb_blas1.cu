@@ -45,6 +45,12 @@ bool debug_enabled() {
   return on == 1;
 }
 
+bool pdl_enabled() {
+  static int on = -1;
+  if (on < 0) { const char* e = std::getenv("FB_PDL"); on = (e && e[0] == '1') ? 1 : 0; }
+  return on == 1;
+}
+
 bool check_enabled() {
   static int on = -1;
   if (on < 0) { const char* e = std::getenv("FB_CHECK"); on = ((e && e[0] == '1') || debug_enabled()) ? 1 : 0; }

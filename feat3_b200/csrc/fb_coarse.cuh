@@ -179,6 +179,9 @@ __device__ __forceinline__ double cluster_sum(double v, double* scratch, double*
 template<typename T, int DIM, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
   namespace cgr = cooperative_groups;
+  pdl_wait();
+  // the cluster uses 16 SMs: let the next kernel's CTAs take the others (they wait for us)
+  pdl_trigger();
   cgr::cluster_group cl = cgr::this_cluster();
   __shared__ double sh[THREADS / 32];
   const uint32_t gt = cl.block_rank() * THREADS + threadIdx.x;

@@ -23,6 +23,16 @@ bool check_enabled();
 cudaError_t debug_sync(cudaStream_t s, const char* file, int line);
 void debug_report(cudaError_t e, const char* what, const char* file, int line);
 
+// Programmatic dependent launch: kernels of the solve path may be scheduled while their
+// predecessor in the stream finishes. Every kernel launched that way starts with pdl_wait()
+// (returns once the predecessor has completed and its writes are visible; a no-op for a
+// normal launch), and signals pdl_trigger() when the rest of its work no longer delays the
+// launch of its successor. Off by default (no gain measured on the graph-replayed solve);
+// FB_PDL=1 in the environment turns the attribute on.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+bool pdl_enabled();
+
 // map a CUDA error onto the C-ABI status
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? FB_OK : FB_ERR_CUDA; }
 #define FB_CHECK_LAUNCH() do { cudaError_t _e = cudaGetLastError(); if (_e != cudaSuccess) return FB_ERR_CUDA; } while (0)

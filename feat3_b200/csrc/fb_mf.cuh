@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr uint64_t E = 16 / sizeof(T);
+  pdl_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[NST], empty[NST];
   __shared__ double sh[16];
@@ -457,6 +458,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
       if (lane == 0) mbar_arrive(&empty[s]);
     }
   }
+  pdl_trigger();
   if (Epi::kReduce) {
     const double blk = block_sum<288>(acc, sh);
     reduce_finish<288>(blk, ws, counter, red_out, sh, false);

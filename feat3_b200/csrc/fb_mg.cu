@@ -46,6 +46,22 @@ static int occupancy_grid(const void* fn, uint64_t work_warps) {
   return int(g < 1 ? 1 : g);
 }
 
+// launch with the programmatic-dependent-launch attribute (the kernel begins with pdl_wait())
+template<typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(cudaStream_t s, void (*fn)(KArgs...), dim3 grid, dim3 block, size_t smem, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, fn, static_cast<KArgs>(args)...);
+}
+
 // ------------------------------------------------------------------ launch helpers
 // debugging aid (FB_DEBUG=1): report pointers that are not device memory of this context
 static void debug_check_ptrs(const char* what, std::initializer_list<const void*> ptrs) {
@@ -242,6 +258,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
                                                     double* ws, unsigned* counter, double* rr_out,
                                                     void* s1, const void* invd, const uint32_t* mask, double omega) {
   using T = typename std::conditional<LOW, float, double>::type;
+  pdl_wait();
   __shared__ double sh[8];
   // alpha = gamma' / (q . p) with gamma' = r . z of this iteration (pcg.hpp:241-251); the thread
   // that finishes the reduction then commits gamma <- gamma' for the next direction update
@@ -262,6 +279,7 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
     if (s1t) s1t[i] = masked(mask, i) ? T(0) : om * (invt[i] * T(ri));
     acc += ri * ri;
   }
+  pdl_trigger();
   const double blk = block_sum<256>(acc, sh);
   if (reduce_finish<256>(blk, ws, counter, rr_out, sh, false)) sc->gamma = sc->rz;
 }
@@ -270,10 +288,12 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
 template<typename ZT>
 __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, const ZT* __restrict__ z, uint32_t n,
                                                 double* ws, unsigned* counter, double* out) {
+  pdl_wait();
   __shared__ double sh[8];
   double acc = 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     acc += r[i] * double(z[i]);
+  pdl_trigger();
   const double blk = block_sum<256>(acc, sh);
   reduce_finish<256>(blk, ws, counter, out, sh, false);
 }
@@ -281,6 +301,7 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
 // p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update
 template<typename ZT>
 __global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+  pdl_wait();
   const double beta = sc->rz / sc->gamma;
   const bool upd = fabs(beta) >= eps_of<double>();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -422,7 +443,8 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
   G.dyt = grid % G.tpp;
   const T* s0 = NS > 0 ? static_cast<const T*>(SE::stream(epi, 0)) : nullptr;
   const T* s1 = NS > 1 ? static_cast<const T*>(SE::stream(epi, 1)) : nullptr;
-  fn<<<grid, 288, dyn, m->stream>>>(v, G, x, epi, s0, s1, mask, m->ws, m->counter, red_out, m->kerr);
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(288), dyn, v, G, x, epi, s0, s1, mask, m->ws, m->counter, red_out,
+                     m->kerr));
   m->launches++;
   FB_CHECK_LAUNCH();
   return FB_OK;
@@ -449,7 +471,8 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   if (debug_enabled())
     debug_check_ptrs("k_mf_q1", {(const void*)v.k, (const void*)x, (const void*)m->ws, (const void*)m->counter,
                                  (const void*)red_out});
-  fn<<<occupancy_grid((const void*)fn, v.nchunks), 256, 0, m->stream>>>(v, x, epi, m->ws, m->counter, red_out);
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(occupancy_grid((const void*)fn, v.nchunks)), dim3(256), 0, v, x, epi, m->ws,
+                     m->counter, red_out));
   m->launches++;
   FB_CHECK_LAUNCH();
   if (v.err && debug_enabled()) FB_TRY(check_self_checks(m));
@@ -486,7 +509,7 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
       if (L.tr.dim == 3) {
         constexpr int CZ = sizeof(T) == 4 ? 4 : 2;  // static shared tile below 48 KB
         const dim3 grid((L.tr.Mc1 + 31) / 32, (L.tr.Mc1 + 7) / 8, (L.tr.Mc1 + CZ - 1) / CZ);
-        k_rest_q1_tile<T, CZ><<<grid, 256, 0, m->stream>>>(L.tr, xf, epi, m->ws, m->counter, red);
+        FB_CUDA(launch_pdl(m->stream, k_rest_q1_tile<T, CZ>, grid, dim3(256), 0, L.tr, xf, epi, m->ws, m->counter, red));
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
@@ -512,7 +535,7 @@ static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
         constexpr int FZ = 16;
         const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + FZ - 1) / FZ);
         const int bmask = L.mask_boundary && epi.mask == L.mask;
-        k_prol_q1_tile<T, FZ><<<grid, 256, 0, m->stream>>>(L.tr, xc, epi.sol, epi.mask, bmask);
+        FB_CUDA(launch_pdl(m->stream, k_prol_q1_tile<T, FZ>, grid, dim3(256), 0, L.tr, xc, epi.sol, epi.mask, bmask));
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
@@ -630,11 +653,13 @@ static int launch_coarse(fb_mg* m, int lc, T** sol_lc) {
   cfg.gridDim = dim3(cs);
   cfg.blockDim = dim3(coarse_threads<T>());
   cfg.stream = m->stream;
-  cudaLaunchAttribute at;
-  at.id = cudaLaunchAttributeClusterDimension;
-  at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
-  cfg.attrs = &at;
-  cfg.numAttrs = 1;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs; at[0].val.clusterDim.y = 1; at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
   if (m->dim == 3) FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 3, coarse_threads<T>()>, A));
   else FB_CUDA(cudaLaunchKernelEx(&cfg, k_coarse_cycle<T, 2, coarse_threads<T>()>, A));
   m->launches++;
@@ -823,25 +848,31 @@ static int body(fb_mg* m) {
   if (m->cfg.outer == FB_OUTER_PCG) {
     // gamma' = r . z ; p = z + beta p ; q = A p ; x, r update
     if (!dot_done) {
-      if (low) k_dot_rz<float><<<occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz);
-      else     k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, m->stream>>>(m->r, (const double*)z, n, m->ws, m->counter, &m->sc->rz);
+      if (low) FB_CUDA(launch_pdl(m->stream, k_dot_rz<float>, dim3(occupancy_grid((const void*)k_dot_rz<float>, n / 32 + 1)),
+                                  dim3(256), 0, (const double*)m->r, (const float*)z, n, m->ws, m->counter, &m->sc->rz));
+      else     FB_CUDA(launch_pdl(m->stream, k_dot_rz<double>, dim3(occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1)),
+                                  dim3(256), 0, (const double*)m->r, (const double*)z, n, m->ws, m->counter, &m->sc->rz));
       m->launches++;
       FB_CHECK_LAUNCH();
     }
-    if (low) k_pcg_dir<float><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const float*)z, m->sc, n);
-    else     k_pcg_dir<double><<<ew_grid(n), 256, 0, m->stream>>>(m->p, (const double*)z, m->sc, n);
+    if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, (const float*)z,
+                                (const DevScalars*)m->sc, n));
+    else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir<double>, dim3(ew_grid(n)), dim3(256), 0, m->p, (const double*)z,
+                                (const DevScalars*)m->sc, n));
     m->launches++;
     FB_CHECK_LAUNCH();
     EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
     FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
     Level& L0 = m->L[0];
     const bool fs = fuse_s1(m);
-    if (low) k_pcg_update<true><<<occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1), 256, 0, m->stream>>>(
-        m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x32 : nullptr,
-        L0.invd32, L0.mask, m->cfg.omega_rich);
-    else     k_pcg_update<false><<<occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1), 256, 0, m->stream>>>(
-        m->xb, m->r, m->r32, m->p, m->q, m->sc, n, m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x64 : nullptr,
-        L0.invd64, L0.mask, m->cfg.omega_rich);
+    if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_update<true>, dim3(occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1)),
+                                dim3(256), 0, m->xb, m->r, m->r32, (const double*)m->p, (const double*)m->q, m->sc, n,
+                                m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x32 : nullptr, (const void*)L0.invd32,
+                                (const uint32_t*)L0.mask, m->cfg.omega_rich));
+    else     FB_CUDA(launch_pdl(m->stream, k_pcg_update<false>, dim3(occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1)),
+                                dim3(256), 0, m->xb, m->r, m->r32, (const double*)m->p, (const double*)m->q, m->sc, n,
+                                m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x64 : nullptr, (const void*)L0.invd64,
+                                (const uint32_t*)L0.mask, m->cfg.omega_rich));
     m->launches++;
     FB_CHECK_LAUNCH();
   } else {

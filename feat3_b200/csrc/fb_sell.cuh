@@ -388,6 +388,7 @@ __global__ void __launch_bounds__(256) k_mf_q1(MfView<T, DIM> A, const T* __rest
                                                double* ws, unsigned* counter, double* red_out) {
   constexpr int S = DIM == 3 ? 27 : 9;
   constexpr int NE = 1 << DIM;
+  pdl_wait();
   __shared__ double sh[8];
   const int lane = threadIdx.x & 31;
   const uint32_t wpb = blockDim.x >> 5;
@@ -451,6 +452,7 @@ __global__ void __launch_bounds__(256) k_mf_q1(MfView<T, DIM> A, const T* __rest
     }
     if (row <= last) acc += epi(uint32_t(row), s);
   }
+  pdl_trigger();
   if (Epi::kReduce) {
     const double blk = block_sum<256>(acc, sh);
     reduce_finish<256>(blk, ws, counter, red_out, sh, false);
@@ -686,6 +688,7 @@ __global__ void __launch_bounds__(256) k_rest_q1_3d(Q1Transfer g, const T* __res
       acc += epi(i, s);
     }
   }
+  pdl_trigger();
   const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
   const double blk = block_sum_tid<256>(acc, sh, tid);
   const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
@@ -702,6 +705,7 @@ template<typename T, int CZ>
 __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __restrict__ xf, EpiRestrict<T> epi,
                                                       double* ws, unsigned* counter, double* red_out) {
   constexpr int SX = 65, SY = 17, SZ = 2 * CZ + 1;
+  pdl_wait();
   __shared__ T sm[SZ][SY][SX];
   __shared__ double sh[8];
   const int X0 = int(blockIdx.x) * 32, Y0 = int(blockIdx.y) * 8, Z0 = int(blockIdx.z) * CZ;
@@ -783,6 +787,7 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
                                                       const uint32_t* __restrict__ mask, int bmask) {
   static_assert(FZ % 2 == 0, "slabs start on even planes");
   constexpr int CX = 17, CY = 5, CZ = FZ / 2 + 1;
+  pdl_wait();
   __shared__ T cm[CZ][CY][CX];
   const uint32_t X0 = blockIdx.x * 32, Y0 = blockIdx.y * 8, Z0 = blockIdx.z * FZ;
   const uint32_t cx0 = X0 >> 1, cy0 = Y0 >> 1, cz0 = Z0 >> 1;
@@ -808,6 +813,7 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
     }
   }
   __syncthreads();
+  pdl_trigger();
   if (!act) return;
   const bool bxy = X == 0 || X == g.Mf1 - 1 || Y == 0 || Y == g.Mf1 - 1;
   const uint32_t lx0 = (X >> 1) - cx0, lx1 = ((X + 1) >> 1) - cx0;
