@@ -176,11 +176,12 @@ __device__ __forceinline__ void widen(uint64_t lo, uint64_t hi, uint64_t& alo, u
 }
 
 // ------------------------------------------------------------------ direct-path row
-// A(k) x for one row with clamped gathers (any row of the level)
+// A(k) x for one row at lattice point (X, Y, Z) with clamped gathers (any row of the level)
 template<typename T>
-__device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __restrict__ x, int32_t row) {
+__device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __restrict__ x, int32_t row, int32_t X,
+                                           int32_t Y, int32_t Z) {
   const int32_t last = int32_t(A.rows) - 1;
-  const int32_t M1 = int32_t(A.M1), N = M1 - 1;
+  const int32_t N = int32_t(A.M1) - 1;
   T xv[27];
 #pragma unroll
   for (int j = 0; j < 27; ++j) {
@@ -188,7 +189,6 @@ __device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __res
     col = col < 0 ? 0 : (col > last ? last : col);
     xv[j] = __ldg(x + col);
   }
-  const int32_t X = row % M1, t = row / M1, Y = t % M1, Z = t / M1;
   T s = T(0);
 #pragma unroll
   for (int e = 0; e < 8; ++e) {
@@ -321,21 +321,24 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
       const uint32_t nitems = G.nbl_items + G.nedge_items;
       for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
         int32_t row = -1;
+        uint32_t X = 0, Y = 0, Z = 0;
         if (item < G.nbl_items) {
-          const uint32_t bl = item / cpl, X = (item % cpl) * 32 + lane;
-          uint32_t Y, Z;
-          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl % M1; }
-          else { const uint32_t r = bl - 2 * M1; Z = 1 + r / 2; Y = (r & 1) ? M1 - 1 : 0; }
+          const uint32_t bl = item / cpl;
+          X = (item - bl * cpl) * 32 + lane;
+          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl < M1 ? bl : bl - M1; }
+          else { const uint32_t r = bl - 2 * M1; Z = 1 + (r >> 1); Y = (r & 1) ? M1 - 1 : 0; }
           if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
         } else {
           const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
           if (li < W * W) {
-            const uint32_t Y = 1 + li % W, Z = 1 + li / W;
-            row = int32_t((Z * M1 + Y) * M1 + ((lane & 1) ? M1 - 1 : 0));
+            const uint32_t zq = li / W;
+            Y = 1 + (li - zq * W); Z = 1 + zq;
+            X = (lane & 1) ? M1 - 1 : 0;
+            row = int32_t((Z * M1 + Y) * M1 + X);
           }
         }
         if (row >= 0) {
-          const T s = mf_row_direct<T>(A, x, row);
+          const T s = mf_row_direct<T>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
           acc += epi(uint32_t(row), s);
         }
       }
@@ -346,14 +349,12 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
     const uint32_t grp = tid / W, X = 1 + (tid - grp * W);
     const bool active = grp < G.G;
     uint32_t it = 0;
-    bool ok = true;
     TileIter ti(G, blockIdx.x);
     for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it, ti.next(G)) {
       const int s = int(it % NST);
       const uint32_t ph = (it / NST) & 1u;
       if (!mbar_wait(&full[s], ph)) {
         atomicExch(kerr, 3u);
-        ok = false;
         break;
       }
       const TileGeo g = tile_geo(G, ti);
@@ -404,10 +405,15 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
           for (int q = 0; q < 3; ++q)
 #pragma unroll
             for (int d = 0; d < 3; ++d) xw[q][2][d] = xs[q][(j + 2) * int(M1) + d - 1];
+          if (A.k) {
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            kw[q][1][0] = A.k ? ks[q][(j + 1) * N] : T(1);
-            kw[q][1][1] = A.k ? ks[q][(j + 1) * N + 1] : T(1);
+            for (int q = 0; q < 2; ++q) {
+              kw[q][1][0] = ks[q][(j + 1) * N];
+              kw[q][1][1] = ks[q][(j + 1) * N + 1];
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) kw[q][1][0] = kw[q][1][1] = T(1);
           }
           // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
           // sum of k over the cells holding both the row's node and d, where r(d) has a bit for

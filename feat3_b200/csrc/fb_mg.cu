@@ -401,14 +401,13 @@ static int check_self_checks(fb_mg* m) {
 }
 
 // line-tiled staged launch (3D levels with at least 16 interior points per line)
-template<typename T, typename Epi>
-static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
-                           double* red_out) {
+template<typename T, typename Epi, int TY>
+static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
+                              double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr int NST = 2;
   constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
-  constexpr int TY = sizeof(T) == 4 ? 4 : 3;
   const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
   // a structured level's filter is its lattice boundary, which no tile row touches
@@ -448,6 +447,14 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
   m->launches++;
   FB_CHECK_LAUNCH();
   return FB_OK;
+}
+
+// lines per thread: 4 (FP32) / 3 (FP64); 2 lines on the smaller FP32 levels (more tiles per CTA)
+// measured no faster
+template<typename T, typename Epi>
+static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
+                           double* red_out) {
+  return launch_mf_tiled_ty<T, Epi, sizeof(T) == 4 ? 4 : 3>(m, L, v, x, epi, red_out);
 }
 
 template<typename T, typename Epi, int DIM>

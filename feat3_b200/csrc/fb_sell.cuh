@@ -571,131 +571,6 @@ __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restri
   }
 }
 
-// 3D prolongation + coarse-grid correction (EpiProlong: sol += filter_cor(P x_c)) for ZB
-// consecutive fine planes per thread, launched on a (ceil(Mf1/32), ceil(Mf1/8), ceil(Mf1/ZB))
-// grid of 32x8 blocks. The ZB/2+1 coarse planes behind the slab are read once, and all
-// iterate values of the slab are loaded before the first store, so a thread keeps ~30
-// independent loads in flight. Per fine point the terms and their order are those of
-// k_prol_q1 (the CSR row order plus exact zeros).
-template<typename T, int ZB>
-__global__ void __launch_bounds__(256) k_prol_q1_3d(Q1Transfer g, const T* __restrict__ xc, T* __restrict__ sol,
-                                                    const uint32_t* __restrict__ mask) {
-  static_assert(ZB % 2 == 0, "slabs start on even planes");
-  const uint32_t X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z0 = blockIdx.z * ZB;
-  if (X >= g.Mf1 || Y >= g.Mf1) return;
-  const uint32_t cx0 = X >> 1, cx1 = (X + 1) >> 1, cy0 = Y >> 1, cy1 = (Y + 1) >> 1;
-  constexpr int NQ = ZB / 2 + 1;
-  T v[NQ][4];
-#pragma unroll
-  for (int q = 0; q < NQ; ++q) {
-    uint32_t cz = Z0 / 2 + q;
-    cz = cz < g.Mc1 ? cz : g.Mc1 - 1;  // planes past the lattice feed no fine point
-    const size_t r0 = (size_t(cz) * g.Mc1 + cy0) * g.Mc1, r1 = (size_t(cz) * g.Mc1 + cy1) * g.Mc1;
-    v[q][0] = xc[r0 + cx0]; v[q][1] = xc[r0 + cx1];
-    v[q][2] = xc[r1 + cx0]; v[q][3] = xc[r1 + cx1];
-  }
-  const size_t plane = size_t(g.Mf1) * g.Mf1;
-  const size_t i0 = X + size_t(g.Mf1) * (Y + size_t(g.Mf1) * Z0);
-  T old[ZB];
-  uint32_t mw[ZB];
-#pragma unroll
-  for (int z = 0; z < ZB; ++z) {
-    const bool in = Z0 + z < g.Mf1;
-    const size_t i = in ? i0 + z * plane : i0;
-    old[z] = sol[i];
-    mw[z] = mask ? __ldg(mask + (i >> 5)) : 0u;
-  }
-  const T hx = (X & 1) ? T(0.5) : T(1), hy = (Y & 1) ? T(0.5) : T(1);
-  const T wy1 = (Y & 1) ? T(1) : T(0);
-#pragma unroll
-  for (int z = 0; z < ZB; ++z) {
-    if (Z0 + z >= g.Mf1) break;
-    const size_t i = i0 + z * plane;
-    const T w = hx * hy * ((z & 1) ? T(0.5) : T(1));
-    const T wx1 = (X & 1) ? w : T(0);
-    const T wz1 = (z & 1) ? T(1) : T(0);
-    const int q0 = z >> 1, q1 = (z + 1) >> 1;
-    T s = T(0);
-    s += w * v[q0][0];
-    s += wx1 * v[q0][1];
-    s += (wy1 * w) * v[q0][2];
-    s += (wy1 * wx1) * v[q0][3];
-    s += (wz1 * w) * v[q1][0];
-    s += (wz1 * wx1) * v[q1][1];
-    s += (wz1 * wy1 * w) * v[q1][2];
-    s += (wz1 * wy1 * wx1) * v[q1][3];
-    if (!((mw[z] >> (i & 31)) & 1u)) sol[i] = T(1) * s + old[z];
-  }
-}
-
-// 3D restriction (EpiRestrict: rhs_c = filter_def(R d), ||rhs_c||^2, optional first
-// pre-smoothing step sol1 = omega filter_cor(invd o rhs_c)) for ZB consecutive coarse planes
-// per thread; fine plane 2Zc+1 is shared by coarse planes Zc and Zc+1 and read once.
-// Launched on a (ceil(Mc1/32), ceil(Mc1/8), ceil(Mc1/ZB)) grid of 32x8 blocks. Per coarse
-// point the terms and their order are those of k_rest_q1.
-template<typename T, int ZB>
-__global__ void __launch_bounds__(256) k_rest_q1_3d(Q1Transfer g, const T* __restrict__ xf, EpiRestrict<T> epi,
-                                                    double* ws, unsigned* counter, double* red_out) {
-  __shared__ double sh[8];
-  const int X = int(blockIdx.x * 32 + threadIdx.x), Y = int(blockIdx.y * 8 + threadIdx.y);
-  const int Zc0 = int(blockIdx.z) * ZB;
-  double acc = 0.0;
-  if (X < int(g.Mc1) && Y < int(g.Mc1)) {
-    const int F = int(g.Mf1) - 1;
-    int fx[3], fy[3];
-    T wx[3], wy[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int ox = 2 * X + d - 1, oy = 2 * Y + d - 1;
-      const T wd = d == 1 ? T(1) : T(0.5);
-      wx[d] = (ox < 0 || ox > F) ? T(0) : wd;
-      wy[d] = (oy < 0 || oy > F) ? T(0) : wd;
-      fx[d] = ox < 0 ? 0 : (ox > F ? F : ox);
-      fy[d] = oy < 0 ? 0 : (oy > F ? F : oy);
-    }
-    // fine planes 2*Zc0-1 .. 2*Zc0+2*ZB-1 (clamped), 9 values each
-    constexpr int NP = 2 * ZB + 1;
-    T v[NP][9];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-      int oz = 2 * Zc0 - 1 + p;
-      oz = oz < 0 ? 0 : (oz > F ? F : oz);
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        const T* row = xf + (size_t(oz) * g.Mf1 + fy[b]) * g.Mf1;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[p][b * 3 + c] = row[fx[c]];
-      }
-    }
-#pragma unroll
-    for (int zc = 0; zc < ZB; ++zc) {
-      const int Z = Zc0 + zc;
-      if (Z >= int(g.Mc1)) break;
-      T wz[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const int oz = 2 * Z + d - 1;
-        wz[d] = (oz < 0 || oz > F) ? T(0) : (d == 1 ? T(1) : T(0.5));
-      }
-      T s = T(0);
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) s += (wx[c] * wy[b] * wz[a]) * v[2 * zc + a][b * 3 + c];
-      const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
-      acc += epi(i, s);
-    }
-  }
-  pdl_trigger();
-  const uint32_t tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const double blk = block_sum_tid<256>(acc, sh, tid);
-  const uint32_t nblk = gridDim.x * gridDim.y * gridDim.z;
-  const uint32_t bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  reduce_finish_nd<256>(blk, ws, counter, red_out, sh, bid, nblk);
-}
-
 // 3D restriction with the fine block staged in shared memory: a block owns 32 x 8 x CZ coarse
 // points and first loads the (65 x 17 x (2 CZ + 1)) fine values around them with coalesced
 // loads (indices clamped; a clamped value always meets weight 0), then every thread forms CZ
