@@ -432,19 +432,25 @@ struct MG {
     }
   }
 
-  // MultiGrid::apply with a V-cycle (multigrid.hpp:1268-1350, 1524-1587, 1711-2000)
-  void vcycle(T* cor_out, const T* def_in) {
-    const int64_t n0 = L[0].A.rows;
-    std::copy(def_in, def_in + n0, L[0].rhs.begin());
-    for (int i = 0; i + 1 < nl; ++i) {
+  // restriction from level cur down to the coarse level (multigrid.hpp:1711-1832): the
+  // pre-smoother (from zero) runs on every level below cur, and on cur itself only when
+  // cur_smooth; otherwise the defect left by the peak smoother is restricted
+  void apply_rest(int cur, bool cur_smooth) {
+    for (int i = cur; i + 1 < nl; ++i) {
       MGLevel<T>& f = L[i];
       MGLevel<T>& c = L[i + 1];
-      smooth(f, f.sol.data(), f.rhs.data());
-      csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+      if (cur_smooth || i > cur) {
+        smooth(f, f.sol.data(), f.rhs.data());
+        csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+      }
       filter_zero(f.def.data(), *f.filt);
       csr_apply(c.rhs.data(), T(1), f.def.data(), T(0), c.rhs.data(), f.R);
       filter_zero(c.rhs.data(), *c.filt);
     }
+  }
+
+  // coarse-grid solve on the coarsest level (multigrid.hpp:1524-1587)
+  void apply_coarse() {
     MGLevel<T>& cl = L[nl - 1];
     switch (cfg.coarse) {
       case 0: apply_direct(cl, cl.sol.data(), cl.rhs.data()); break;
@@ -454,17 +460,89 @@ struct MG {
         std::copy(cl.rhs.begin(), cl.rhs.end(), cl.sol.begin());
         filter_zero(cl.sol.data(), *cl.filt);
     }
-    for (int i = nl - 2; i >= 0; --i) {
+  }
+
+  // prolongation from the coarse level up to level cur (multigrid.hpp:1843-2000), with the
+  // fixed (omega = 1) or adaptive coarse-grid correction and post-smoothing on every level
+  // above cur, on cur itself only when cur_smooth
+  void apply_prol(int cur, bool cur_smooth) {
+    for (int i = nl - 2; i >= cur; --i) {
       MGLevel<T>& f = L[i];
       MGLevel<T>& c = L[i + 1];
       const int64_t n = f.A.rows;
       csr_apply(f.cor.data(), T(1), c.sol.data(), T(0), f.cor.data(), f.P);
       filter_zero(f.cor.data(), *f.filt);
-      axpy(f.sol.data(), f.cor.data(), f.sol.data(), T(1), n);
-      csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
-      filter_zero(f.def.data(), *f.filt);
-      smooth(f, f.cor.data(), f.def.data());
-      axpy(f.sol.data(), f.cor.data(), f.sol.data(), T(1), n);
+      T omega = T(1);
+      if (cfg.cgc != 0) {
+        csr_apply(f.tmp.data(), T(1), f.cor.data(), T(0), f.tmp.data(), f.A);
+        filter_zero(f.tmp.data(), *f.filt);
+        if (cfg.cgc == 1) omega = dot(f.def.data(), f.cor.data(), n) / dot(f.tmp.data(), f.cor.data(), n);
+        else omega = dot(f.def.data(), f.tmp.data(), n) / dot(f.tmp.data(), f.tmp.data(), n);
+      }
+      axpy(f.sol.data(), f.cor.data(), f.sol.data(), omega, n);
+      if (cur_smooth || i > cur) {
+        if (cfg.cgc != 0) {
+          axpy(f.def.data(), f.tmp.data(), f.def.data(), -omega, n);
+        } else {
+          csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+          filter_zero(f.def.data(), *f.filt);
+        }
+        smooth(f, f.cor.data(), f.def.data());
+        axpy(f.sol.data(), f.cor.data(), f.sol.data(), T(1), n);
+      }
+    }
+  }
+
+  // peak smoother on level l (multigrid.hpp:1589-1680): defect, one application of the
+  // level's (peak = pre = post) smoother to it, correction, defect again
+  void smooth_peak(int l) {
+    MGLevel<T>& f = L[l];
+    const int64_t n = f.A.rows;
+    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+    filter_zero(f.def.data(), *f.filt);
+    smooth(f, f.cor.data(), f.def.data());
+    filter_zero(f.cor.data(), *f.filt);
+    axpy(f.sol.data(), f.cor.data(), f.sol.data(), T(1), n);
+    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+    filter_zero(f.def.data(), *f.filt);
+  }
+
+  // MultiGrid::apply (multigrid.hpp:1268-1519): V, F or W cycle
+  void vcycle(T* cor_out, const T* def_in) {
+    const int64_t n0 = L[0].A.rows;
+    std::copy(def_in, def_in + n0, L[0].rhs.begin());
+    const int last = nl - 1;
+    if (cfg.cycle == 1) {
+      apply_rest(0, true);
+      for (int peak = last - 1; peak > 0; --peak) {
+        apply_coarse();
+        apply_prol(peak, false);
+        smooth_peak(peak);
+        apply_rest(peak, false);
+      }
+      apply_coarse();
+      apply_prol(0, true);
+    } else if (cfg.cycle == 2) {
+      apply_rest(0, true);
+      apply_coarse();
+      std::vector<int> cnt(nl, 0);
+      const int num_cgs = 1 << last;
+      for (int cgs = 1; cgs < num_cgs; ++cgs) {
+        int peak = last;
+        while (peak > 0)
+          if (cnt[--peak] == 0) break;
+        for (int i = last - 1; i > peak; --i) cnt[i] = 0;
+        ++cnt[peak];
+        apply_prol(peak, false);
+        smooth_peak(peak);
+        apply_rest(peak, false);
+        apply_coarse();
+      }
+      apply_prol(0, true);
+    } else {
+      apply_rest(0, true);
+      apply_coarse();
+      apply_prol(0, true);
     }
     std::copy(L[0].sol.begin(), L[0].sol.end(), cor_out);
   }

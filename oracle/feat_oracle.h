@@ -64,6 +64,8 @@ typedef struct or_cfg {
   double tol_rel;
   int max_iter;
   int inner;         /* 0 = FP64 multigrid, 1 = FP32 multigrid, 2 = FP32 with FP16-quantised matrices */
+  int cycle;         /* 0 = V, 1 = F, 2 = W (Solver::MultiGridCycle) */
+  int cgc;           /* 0 = fixed, 1 = min-energy, 2 = min-defect (Solver::MultiGridAdaptCGC) */
 } or_cfg;
 
 /* solves A sol = rhs with the configured solver (sol holds the initial guess).
@@ -72,7 +74,7 @@ typedef struct or_cfg {
  * 4 diverged, 5 max_iter, 6 stagnated). */
 int or_solve(const or_hier* h, const or_cfg* cfg, const double* rhs, double* sol, double* hist, int* iters);
 
-/* one V-cycle (preconditioner application) on the finest level: cor = MG(def) */
+/* one multigrid cycle of the configured type (preconditioner application): cor = MG(def) */
 void or_vcycle(const or_hier* h, const or_cfg* cfg, const double* def, double* cor);
 
 /* element gradient on the finest level: grad[e] = -lambda_e^T K_e^(1) u_e */

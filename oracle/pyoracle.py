@@ -67,13 +67,18 @@ def lib():
 class Cfg(C.Structure):
     _fields_ = [("solver", C.c_int), ("nu", C.c_int), ("omega_jac", C.c_double),
                 ("omega_rich", C.c_double), ("omega_outer", C.c_double), ("coarse", C.c_int),
-                ("tol_rel", C.c_double), ("max_iter", C.c_int), ("inner", C.c_int)]
+                ("tol_rel", C.c_double), ("max_iter", C.c_int), ("inner", C.c_int), ("cycle", C.c_int),
+                ("cgc", C.c_int)]
+
+
+CYCLE = {"v": 0, "f": 1, "w": 2}
+CGC = {"fixed": 0, "energy": 1, "defect": 2}
 
 
 def make_cfg(solver="pcg", nu=4, omega_jac=0.5, omega_rich=1.0, omega_outer=1.0, coarse="direct",
-             tol=1e-8, max_iter=1000, inner="f64"):
+             tol=1e-8, max_iter=1000, inner="f64", cycle="v", cgc="fixed"):
     return Cfg(0 if solver == "pcg" else 1, nu, omega_jac, omega_rich, omega_outer, COARSE[coarse],
-               tol, max_iter, INNER[inner])
+               tol, max_iter, INNER[inner], CYCLE[cycle], CGC[cgc])
 
 
 def _p(a):
@@ -197,7 +202,7 @@ def _read_info(fn):
 
 def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", nu=4, omega_jac=0.5,
             omega_rich=1.0, omega_outer=1.0, coarse="direct", tol=1e-8, max_iter=1000, inner="f64",
-            target=None, dump_matrices=False, workdir=None):
+            target=None, dump_matrices=False, workdir=None, cycle="v", cgc="fixed"):
     """Run the reference's own FP64/mixed MG solver; returns info and arrays in lattice order."""
     if not have_ref():
         raise FileNotFoundError(REF_BIN)
@@ -207,7 +212,8 @@ def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", n
            "--level-min", str(level_min), "--rhs", rhs, "--solver", solver, "--nu", str(nu),
            "--omega-jac", repr(omega_jac), "--omega-rich", repr(omega_rich),
            "--omega-outer", repr(omega_outer), "--coarse", coarse, "--tol", repr(tol),
-           "--maxit", str(max_iter), "--inner", inner, "--out", out, "--quiet"]
+           "--maxit", str(max_iter), "--inner", inner, "--out", out, "--quiet", "--cycle", cycle,
+           "--cgc", cgc]
     if k is not None:
         kf = os.path.join(wd, "k.bin")
         np.ascontiguousarray(k, np.float64).tofile(kf)

@@ -83,6 +83,8 @@ namespace RefDriver
     double tol = 1e-8;
     int maxit = 1000;
     std::string inner = "f64";     // f64 | f32 | f16 (mixed: FP64 outer, ConvertPrecond to FP32 MG)
+    std::string cycle = "v";       // v | f | w (Solver::MultiGridCycle)
+    std::string cgc = "fixed";     // fixed | energy | defect (Solver::MultiGridAdaptCGC)
     std::string target;            // adjoint: u_target in lexicographic DOF lattice order
     std::string out = "ref";
     bool dump_matrices = false;
@@ -597,6 +599,20 @@ namespace RefDriver
       if(!cfg.quiet) s.set_plot_mode(Solver::PlotMode::iter);
     }
 
+    // MultiGrid with the configured cycle and coarse-grid correction (multigrid.hpp:1066, 1089-1104)
+    template<typename H_>
+    auto make_multigrid(std::shared_ptr<H_> hier) const
+      -> decltype(Solver::new_multigrid(hier, Solver::MultiGridCycle::V))
+    {
+      Solver::MultiGridCycle cyc = Solver::MultiGridCycle::V;
+      if(cfg.cycle == "f") cyc = Solver::MultiGridCycle::F;
+      else if(cfg.cycle == "w") cyc = Solver::MultiGridCycle::W;
+      auto mg = Solver::new_multigrid(hier, cyc);
+      if(cfg.cgc == "energy") mg->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinEnergy);
+      else if(cfg.cgc == "defect") mg->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinDefect);
+      return mg;
+    }
+
     template<typename M_, typename F_, typename T_, typename LvlGet_>
     std::shared_ptr<Solver::MultiGridHierarchy<M_, F_, T_>> build_hierarchy(LvlGet_ get) const
     {
@@ -632,7 +648,7 @@ namespace RefDriver
       Level& top = *levels.front();
       auto hier = build_hierarchy<MatrixType, FilterType, TransferType>(
         [](Level& l) { return std::tie(l.matrix, l.filter, l.transfer); });
-      auto mgv = Solver::new_multigrid(hier, Solver::MultiGridCycle::V);
+      auto mgv = make_multigrid(hier);
       hier->init();
       if(cfg.solver == "pcg")
       {
@@ -689,7 +705,7 @@ namespace RefDriver
       Level& top = *levels.front();
       auto hier = build_hierarchy<MatrixTypeF, FilterTypeF, TransferTypeF>(
         [](Level& l) { return std::tie(l.matrix_f, l.filter_f, l.transfer_f); });
-      auto mgv = Solver::new_multigrid(hier, Solver::MultiGridCycle::V);
+      auto mgv = make_multigrid(hier);
       auto conv = Solver::new_convert_precond<VectorType, VectorTypeF>(mgv);
       hier->init();
       if(cfg.solver == "pcg")
@@ -815,6 +831,8 @@ int main(int argc, char** argv)
     else if(a == "--tol") cfg.tol = std::atof(next().c_str());
     else if(a == "--maxit") cfg.maxit = std::atoi(next().c_str());
     else if(a == "--inner") cfg.inner = next();
+    else if(a == "--cycle") cfg.cycle = next();
+    else if(a == "--cgc") cfg.cgc = next();
     else if(a == "--target") cfg.target = next();
     else if(a == "--out") cfg.out = next();
     else if(a == "--dump-matrices") cfg.dump_matrices = true;

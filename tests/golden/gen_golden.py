@@ -6,6 +6,7 @@ configuration this project measures and stores its outputs, mapped to the lexico
 lattice numbering through the DOF coordinates, as compressed .npz files:
 
     python tests/golden/gen_golden.py          # needs oracle/_ref/feat_ref
+    python tests/golden/gen_golden.py --cycles # only the F/W-cycle and adaptive-CGC fixtures
 
 Inputs that are random (coefficient fields, target noise) are drawn here with numpy's
 seeded generator and stored in the fixture next to the outputs.
@@ -48,9 +49,28 @@ def run(name, dim, degree, level, level_min, rhs, k=None, keep_u=True, **kw):
     return R
 
 
+def cycles():
+    """F and W cycles and the adaptive coarse-grid corrections (multigrid.hpp:1354-1519, 1898-1925)"""
+    rng = np.random.default_rng(20261204)
+    run("ref_cycle_f_q1_2d_L6", 2, 1, 6, 1, "sine", solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8,
+        cycle="f")
+    k4 = np.exp(rng.standard_normal(16 ** 3))
+    run("ref_cycle_w_q1_3d_L4", 3, 1, 4, 1, "one", k=k4, solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8,
+        cycle="w")
+    run("ref_cgc_energy_q1_2d_L6", 2, 1, 6, 1, "sine", solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8,
+        cgc="energy")
+    k6 = np.exp(0.5 * rng.standard_normal(64 * 64))
+    run("ref_cgc_defect_f_q1_2d_L6", 2, 1, 6, 1, "one", k=k6, solver="pcg", nu=2, omega_jac=0.5, coarse="direct",
+        tol=1e-8, cycle="f", cgc="defect")
+    run("ref_cycle_w_richardson_q1_2d_L5", 2, 1, 5, 1, "sine", solver="richardson", nu=3, omega_jac=0.5,
+        omega_rich=1.0, coarse="smoother", tol=1e-8, cycle="w")
+
+
 def main():
     if not po.have_ref():
         sys.exit("oracle/_ref/feat_ref is missing: build it with `make -C oracle ref` first")
+    if "--cycles" in sys.argv:
+        return cycles()
     rng = np.random.default_rng(20261203)
     # applications/poisson_dirichlet.cpp composition, level 5, the reference's pin (4 +- 1 iterations,
     # applications/CMakeLists.txt:100-108)
