@@ -41,7 +41,7 @@ class CsrHost(C.Structure):
 class SolverCfg(C.Structure):
     _fields_ = [("outer", i32), ("nu", i32), ("omega_jac", dbl), ("omega_rich", dbl), ("omega_outer", dbl),
                 ("coarse", i32), ("tol_rel", dbl), ("max_iter", i32), ("precision", i32), ("use_graphs", i32), ("format", i32),
-                ("flags", i32)]
+                ("flags", i32), ("cycle", i32), ("adapt_cgc", i32)]
 
 
 class SolveInfo(C.Structure):

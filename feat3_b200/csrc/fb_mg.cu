@@ -310,6 +310,52 @@ __global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars*
 
 __global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; }
 
+// adaptive coarse-grid correction factor (multigrid.hpp:1898-1925): MinEnergy
+// omega = (def . cor) / (tmp . cor), MinDefect omega = (def . tmp) / (tmp . tmp), tmp = A cor;
+// both sums in one pass, deterministic (partials per CTA, summed in order by the last CTA)
+template<typename T>
+__global__ void __launch_bounds__(256) k_cgc_omega(const T* __restrict__ def, const T* __restrict__ cor,
+                                                   const T* __restrict__ tmp, uint32_t n, int min_defect,
+                                                   double* ws, unsigned* counter, double* omega) {
+  __shared__ double sh[8];
+  __shared__ bool am_last;
+  double a = 0.0, b = 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double t = double(tmp[i]);
+    if (min_defect) { a += double(def[i]) * t; b += t * t; }
+    else { const double c = double(cor[i]); a += double(def[i]) * c; b += t * c; }
+  }
+  const double ba = block_sum<256>(a, sh);
+  __syncthreads();
+  const double bb = block_sum<256>(b, sh);
+  if (threadIdx.x == 0) {
+    ws[blockIdx.x] = ba;
+    ws[gridDim.x + blockIdx.x] = bb;
+    __threadfence();
+    am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double va = 0.0, vb = 0.0;
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += 256) { va += __ldcg(ws + i); vb += __ldcg(ws + gridDim.x + i); }
+  va = block_sum<256>(va, sh);
+  __syncthreads();
+  vb = block_sum<256>(vb, sh);
+  if (threadIdx.x == 0) {
+    *omega = va / vb;
+    *counter = 0u;
+  }
+}
+
+// sol += omega * cor (the correction is already filtered)
+template<typename T>
+__global__ void k_cgc_update(T* sol, const T* __restrict__ cor, const double* omega, uint32_t n) {
+  const T w = T(*omega);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    sol[i] = w * cor[i] + sol[i];
+}
+
 // Richardson outer: x = omega * z + x
 template<typename ZT>
 __global__ void k_rich_update(double* x, const ZT* __restrict__ z, double omega, uint32_t n) {
@@ -363,6 +409,8 @@ template<> struct Prec<double> {
   static double* y(Level& l) { return l.y64; }
   static double* def(Level& l) { return l.def64; }
   static double* invd(Level& l) { return l.invd64; }
+  static double* cor(Level& l) { return l.cor64; }
+  static double* tmp(Level& l) { return l.tmp64; }
 };
 template<> struct Prec<float> {
   static float* rhs(Level& l) { return l.rhs32; }
@@ -370,6 +418,8 @@ template<> struct Prec<float> {
   static float* y(Level& l) { return l.y32; }
   static float* def(Level& l) { return l.def32; }
   static float* invd(Level& l) { return l.invd32; }
+  static float* cor(Level& l) { return l.cor32; }
+  static float* tmp(Level& l) { return l.tmp32; }
 };
 
 // dispatch a SELL launch on the value storage of the configured precision
@@ -539,7 +589,7 @@ static int prol_T(fb_mg* m, int l, const T* xc, const Epi& epi) {
   if (use_q1_transfer(m, L)) {
     if constexpr (std::is_same<Epi, EpiProlong<T>>::value) {
       if (L.tr.dim == 3) {
-        constexpr int FZ = 16;
+        constexpr int FZ = 8;  // 8 fine planes per thread: measured fastest of 4 / 8 / 16
         const dim3 grid((L.tr.Mf1 + 31) / 32, (L.tr.Mf1 + 7) / 8, (L.tr.Mf1 + FZ - 1) / FZ);
         const int bmask = L.mask_boundary && epi.mask == L.mask;
         FB_CUDA(launch_pdl(m->stream, k_prol_q1_tile<T, FZ>, grid, dim3(256), 0, L.tr, xc, epi.sol, epi.mask, bmask));
@@ -779,6 +829,191 @@ static int vcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** o
   return FB_OK;
 }
 
+// ------------------------------------------------------------------ F and W cycles, adaptive CGC
+// MultiGrid::_apply_cycle_f / _apply_cycle_w (multigrid.hpp:1354-1519) built from the same
+// fused pieces as the V-cycle: restriction from a level with or without its pre-smoothing
+// (_apply_rest), prolongation up to a level with or without its post-smoothing (_apply_prol),
+// with the fixed or adaptive coarse-grid correction, and the peak smoother (_apply_smooth_peak:
+// the level's Richardson smoother on its defect, i.e. nu Jacobi steps from the current
+// iterate, then the defect again). sol[l] tracks which ping-pong buffer holds level l's iterate.
+template<typename T>
+struct Cycle {
+  fb_mg* m;
+  const T* rhs_top;
+  const double* rhs_top_sumsq;
+  std::vector<T*> sol;
+  int nl, nu;
+  T omega;
+  const T* rhs(int l) { return l == 0 ? rhs_top : Prec<T>::rhs(m->L[l]); }
+  const double* bnorm(int l) { return l == 0 ? rhs_top_sumsq : &m->sc->lvl[2 * l]; }
+  T* other(int l, T* cur) { Level& L = m->L[l]; return cur == Prec<T>::x(L) ? Prec<T>::y(L) : Prec<T>::x(L); }
+
+  int defect(int l) {
+    Level& L = m->L[l];
+    EpiDefect<T, false, false> ed{Prec<T>::def(L), rhs(l), L.mask, nullptr};
+    return spmv_L<T>(m, L, sol[l], ed, nullptr);
+  }
+  // nu Jacobi steps from sol[l] (the post-smoother on the defect equation): the first step
+  // reduces the defect norm its successors test (the Richardson smoother's initial-norm test)
+  int smooth_from(int l) {
+    Level& L = m->L[l];
+    T* cur = sol[l];
+    T* oth = other(l, cur);
+    T* s0 = cur;
+    double* dn = &m->sc->lvl[2 * l + 1];
+    for (int it = 0; it < nu; ++it) {
+      if (it == 0) {
+        EpiJacobi<T, true> e{cur, rhs(l), Prec<T>::invd(L), oth, nullptr, L.mask, nullptr, omega};
+        FB_TRY(spmv_L<T>(m, L, cur, e, dn));
+        if (nu == 1) {
+          k_skip_fix<T><<<ew_grid(L.n), 256, 0, m->stream>>>(oth, s0, dn, L.n);
+          m->launches++;
+          FB_CHECK_LAUNCH();
+        }
+      } else {
+        EpiJacobi<T, false> e{cur, rhs(l), Prec<T>::invd(L), oth, s0, L.mask, dn, omega};
+        FB_TRY(spmv_L<T>(m, L, cur, e, nullptr));
+      }
+      std::swap(cur, oth);
+    }
+    sol[l] = cur;
+    return FB_OK;
+  }
+  int rest(int cur, bool cur_smooth) {
+    for (int i = cur; i + 1 < nl; ++i) {
+      Level& L = m->L[i];
+      Level& C = m->L[i + 1];
+      if (cur_smooth || i > cur) {
+        const bool need_s1 = (i == 0) ? !m->top_s1 : nu < 2;
+        FB_TRY(presmooth<T>(m, i, rhs(i), bnorm(i), need_s1, &sol[i]));
+        FB_TRY(defect(i));
+      }
+      const bool coarsest_next = (i + 2 == nl);
+      T* s1 = nullptr;
+      if (nu >= 2 && (!coarsest_next || m->cfg.coarse == FB_COARSE_SMOOTHER)) s1 = Prec<T>::x(C);
+      EpiRestrict<T> er{Prec<T>::rhs(C), s1, Prec<T>::invd(C), C.mask, omega};
+      FB_TRY(rest_T<T>(m, i, Prec<T>::def(L), er, &m->sc->lvl[2 * (i + 1)]));
+    }
+    return FB_OK;
+  }
+  int coarse() {
+    const int l = nl - 1;
+    Level& L = m->L[l];
+    const T* b = rhs(l);
+    switch (m->cfg.coarse) {
+      case FB_COARSE_DIRECT: {
+        const T* cinv;
+        if constexpr (std::is_same<T, double>::value) cinv = m->cinv64; else cinv = m->cinv32;
+        k_dense_solve<T><<<grid_for(uint64_t(L.n) * 32, 256), 256, 0, m->stream>>>(Prec<T>::x(L), cinv, b, L.n);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+      }
+      case FB_COARSE_SMOOTHER:
+        FB_TRY(presmooth<T>(m, l, b, bnorm(l), l == 0 || nu < 2, &sol[l]));
+        break;
+      case FB_COARSE_PCG: {
+        T* w;
+        if constexpr (std::is_same<T, double>::value) w = m->cg64; else w = m->cg32;
+        const uint32_t nc = L.n;
+        k_coarse_cg<T, 512><<<1, 512, 0, m->stream>>>(m->coarse_csr.view(!std::is_same<T, double>::value), b,
+                                                      Prec<T>::x(L), w, w + nc, w + 2 * uint64_t(nc), L.mask, nc, 100);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+      }
+      case FB_COARSE_NONE:
+      default:
+        k_copy_masked<T><<<ew_grid(L.n), 256, 0, m->stream>>>(Prec<T>::x(L), b, L.mask, L.n);
+        m->launches++;
+        FB_CHECK_LAUNCH();
+        sol[l] = Prec<T>::x(L);
+        break;
+    }
+    return FB_OK;
+  }
+  int prol(int cur, bool cur_smooth) {
+    for (int i = nl - 2; i >= cur; --i) {
+      Level& L = m->L[i];
+      if (m->cfg.adapt_cgc == FB_CGC_FIXED) {
+        EpiProlong<T> ep{sol[i], L.mask};
+        FB_TRY(prol_T<T>(m, i, sol[i + 1], ep));
+      } else {
+        // cor = filter_cor(P x_c); tmp = filter_def(A cor); omega from the level's defect
+        EpiFiltered<T> ec{Prec<T>::cor(L), L.mask};
+        FB_TRY(prol_T<T>(m, i, sol[i + 1], ec));
+        EpiFiltered<T> et{Prec<T>::tmp(L), L.mask};
+        FB_TRY(spmv_L<T>(m, L, (const T*)Prec<T>::cor(L), et, nullptr));
+        double* om = &m->sc->tmp[1];
+        k_cgc_omega<T><<<kRedBlocks, 256, 0, m->stream>>>(Prec<T>::def(L), Prec<T>::cor(L), Prec<T>::tmp(L), L.n,
+                                                          m->cfg.adapt_cgc == FB_CGC_MIN_DEFECT ? 1 : 0, m->ws,
+                                                          m->counter, om);
+        k_cgc_update<T><<<ew_grid(L.n), 256, 0, m->stream>>>(sol[i], Prec<T>::cor(L), om, L.n);
+        m->launches += 2;
+        FB_CHECK_LAUNCH();
+      }
+      // post-smoothing; the defect it starts from (rhs - A sol) is formed by its first step,
+      // which equals def - omega * tmp of the adaptive correction up to rounding
+      if (cur_smooth || i > cur) FB_TRY(smooth_from(i));
+    }
+    return FB_OK;
+  }
+  int peak(int l) {
+    FB_TRY(smooth_from(l));
+    return defect(l);
+  }
+};
+
+template<typename T>
+static int mgcycle(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** out_top) {
+  Cycle<T> c;
+  c.m = m; c.rhs_top = rhs_top; c.rhs_top_sumsq = rhs_top_sumsq;
+  c.nl = (int)m->L.size(); c.nu = m->cfg.nu; c.omega = T(m->cfg.omega_rich);
+  c.sol.assign(c.nl, nullptr);
+  const int last = c.nl - 1;
+  FB_TRY(c.rest(0, true));
+  if (m->cfg.cycle == FB_CYCLE_F) {
+    for (int pk = last - 1; pk > 0; --pk) {
+      FB_TRY(c.coarse());
+      FB_TRY(c.prol(pk, false));
+      FB_TRY(c.peak(pk));
+      FB_TRY(c.rest(pk, false));
+    }
+    FB_TRY(c.coarse());
+  } else if (m->cfg.cycle == FB_CYCLE_W) {
+    FB_TRY(c.coarse());
+    // 2^(levels-1) coarse solves; the next peak is the lowest level above the coarse one whose
+    // counter is 0 (multigrid.hpp:1430-1500)
+    std::vector<int> cnt(c.nl, 0);
+    const int num_cgs = 1 << last;
+    for (int cgs = 1; cgs < num_cgs; ++cgs) {
+      int pk = last;
+      while (pk > 0)
+        if (cnt[--pk] == 0) break;
+      for (int i = last - 1; i > pk; --i) cnt[i] = 0;
+      ++cnt[pk];
+      FB_TRY(c.prol(pk, false));
+      FB_TRY(c.peak(pk));
+      FB_TRY(c.rest(pk, false));
+      FB_TRY(c.coarse());
+    }
+  } else {
+    FB_TRY(c.coarse());
+  }
+  FB_TRY(c.prol(0, true));
+  *out_top = c.sol[0];
+  return FB_OK;
+}
+
+// the V-cycle with the fixed correction has its own driver (fused coarse end, r.z inside)
+template<typename T>
+static int mg_apply(fb_mg* m, const T* rhs_top, const double* rhs_top_sumsq, T** out_top) {
+  if (m->cfg.cycle == FB_CYCLE_V && m->cfg.adapt_cgc == FB_CGC_FIXED) return vcycle<T>(m, rhs_top, rhs_top_sumsq, out_top);
+  return mgcycle<T>(m, rhs_top, rhs_top_sumsq, out_top);
+}
+
 // ------------------------------------------------------------------ stopping logic
 // IterativeSolver defaults and tests (kernel/solver/iterative.hpp:216-235, 490-505, 744-832)
 struct Stop {
@@ -812,7 +1047,8 @@ static bool fuse_s1(const fb_mg* m) {
 // ... and its last post-smoothing step forms r . z (z = that step's result, r = the V-cycle's
 // right-hand side: the outer defect, or its FP32 copy in the mixed forms)
 static bool fuse_dot(const fb_mg* m) {
-  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1 && !(m->cfg.flags & FB_FLAG_NO_DOT_FUSION);
+  return m->cfg.outer == FB_OUTER_PCG && m->cfg.nu >= 2 && m->L.size() > 1 && !(m->cfg.flags & FB_FLAG_NO_DOT_FUSION) &&
+         m->cfg.cycle == FB_CYCLE_V && m->cfg.adapt_cgc == FB_CGC_FIXED;
 }
 
 // outer defect r = filter_def(b - A x), ||r||^2, FP32 copy for the mixed V-cycle
@@ -830,11 +1066,11 @@ static int outer_defect(fb_mg* m) {
 static int precond(fb_mg* m, const void** z_out) {
   if (m->cfg.precision == FB_PREC_F64) {
     double* z = nullptr;
-    FB_TRY(vcycle<double>(m, m->r, &m->sc->rr, &z));
+    FB_TRY(mg_apply<double>(m, m->r, &m->sc->rr, &z));
     *z_out = z;
   } else {
     float* z = nullptr;
-    FB_TRY(vcycle<float>(m, m->r32, &m->sc->rr, &z));
+    FB_TRY(mg_apply<float>(m, m->r32, &m->sc->rr, &z));
     *z_out = z;
   }
   return FB_OK;
@@ -895,7 +1131,8 @@ static int body(fb_mg* m) {
 
 static int run_body(fb_mg* m) {
   if (!m->cfg.use_graphs || debug_enabled()) return body(m);
-  const int key = m->cfg.flags * 256 + m->cfg.format * 64 + m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
+  const int key = ((m->cfg.cycle * 4 + m->cfg.adapt_cgc) * 16 + m->cfg.flags) * 256 + m->cfg.format * 64 +
+                  m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
   if (!m->g_body || m->g_body_key != key) {
     if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; }
     cudaGraph_t g = nullptr;
@@ -933,6 +1170,10 @@ static int ensure_vectors(fb_mg* m, int prec) {
     }
     if (!L.invd64) FB_TRY(dalloc(m, &L.invd64, L.n));
     if (low && !L.invd32) FB_TRY(dalloc(m, &L.invd32, L.n));
+    if (m->cfg.adapt_cgc != FB_CGC_FIXED) {
+      if (!low && !L.cor64) { FB_TRY(dalloc(m, &L.cor64, L.n)); FB_TRY(dalloc(m, &L.tmp64, L.n)); }
+      if (low && !L.cor32) { FB_TRY(dalloc(m, &L.cor32, L.n)); FB_TRY(dalloc(m, &L.tmp32, L.n)); }
+    }
     k_invdiag<<<ew_grid(L.n), 256, 0, m->stream>>>(L.invd64, low ? L.invd32 : nullptr, L.diag, m->cfg.omega_jac, L.n);
     FB_CHECK_LAUNCH();
     if (low) {
@@ -1281,13 +1522,15 @@ void fb_solver_cfg_default(fb_solver_cfg* c) {
   c->use_graphs = 1;
   c->format = FB_FORMAT_SELL;
   c->flags = 0;
+  c->cycle = FB_CYCLE_V;
+  c->adapt_cgc = FB_CGC_FIXED;
 }
 
 int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (!m || !c) return FB_ERR_INVALID;
   if (c->nu < 1 || c->nu > 64 || c->max_iter < 0 || !(c->tol_rel >= 0.0) ||
       c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3 ||
-      c->format < 0 || c->format > 2)
+      c->format < 0 || c->format > 2 || c->cycle < 0 || c->cycle > 2 || c->adapt_cgc < 0 || c->adapt_cgc > 2)
     return FB_ERR_INVALID;
   if (c->coarse == FB_COARSE_PCG && !m->coarse_csr.rp) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;

@@ -74,6 +74,8 @@ struct Level {
   uint32_t nfilt = 0;
   double *rhs64 = nullptr, *x64 = nullptr, *y64 = nullptr, *def64 = nullptr;
   float *rhs32 = nullptr, *x32 = nullptr, *y32 = nullptr, *def32 = nullptr;
+  double *cor64 = nullptr, *tmp64 = nullptr;  // adaptive coarse-grid correction: P x_c and A P x_c
+  float *cor32 = nullptr, *tmp32 = nullptr;
   // structured info
   int N = 0;             // cells per side
   uint64_t ne = 0;       // elements

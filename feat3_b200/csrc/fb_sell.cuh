@@ -145,6 +145,18 @@ struct EpiProlong {
   }
 };
 
+// out = filter(s): the prolongated correction (filter_cor) or A times it (filter_def) of the
+// adaptive coarse-grid correction (both filters zero the Dirichlet entries)
+template<typename T>
+struct EpiFiltered {
+  static constexpr bool kReduce = false;
+  T* out; const uint32_t* mask;
+  __device__ __forceinline__ double operator()(uint32_t row, T s) const {
+    out[row] = masked(mask, row) ? T(0) : s;
+    return 0.0;
+  }
+};
+
 // ------------------------------------------------------------------ SELL kernel
 // AT = accumulation type (double for FP64 values, float otherwise)
 template<typename VT, typename XT, typename AT, typename Epi, int UNROLL>

@@ -219,7 +219,15 @@ typedef struct fb_solver_cfg {
   int use_graphs;     /* capture the per-iteration launch sequence in a CUDA graph */
   int format;         /* FB_FORMAT_SELL, FB_FORMAT_STENCIL or FB_FORMAT_MATFREE */
   int flags;          /* FB_FLAG_*: switch individual fusions off (testing; 0 = all on) */
+  int cycle;          /* FB_CYCLE_V, FB_CYCLE_F or FB_CYCLE_W (Solver::MultiGridCycle) */
+  int adapt_cgc;      /* FB_CGC_FIXED, FB_CGC_MIN_ENERGY or FB_CGC_MIN_DEFECT (Solver::MultiGridAdaptCGC) */
 } fb_solver_cfg;
+#define FB_CYCLE_V 0
+#define FB_CYCLE_F 1
+#define FB_CYCLE_W 2
+#define FB_CGC_FIXED 0
+#define FB_CGC_MIN_ENERGY 1
+#define FB_CGC_MIN_DEFECT 2
 /* flags: the coarse end of the V-cycle level by level instead of one cluster launch; PCG's
  * r . z as its own reduction instead of inside the last smoothing step; the matrix-free
  * operator without the shared-memory tiled kernel */

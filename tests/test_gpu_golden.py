@@ -30,7 +30,8 @@ def gpu_solve(fx, fmt="sell", precision="f64", outer=None):
     mg = MultiGrid.structured(int(fx["dim"]), int(fx["degree"]), int(fx["level"]), int(fx["level_min"]), fx.get("k"))
     mg.configure(outer=outer or cfg.get("solver", "pcg"), nu=cfg.get("nu", 4), omega_jac=cfg.get("omega_jac", 0.5),
                  omega_rich=cfg.get("omega_rich", 1.0), coarse=cfg.get("coarse", "direct"), tol=cfg.get("tol", 1e-8),
-                 max_iter=cfg.get("max_iter", 1000), precision=precision, format=fmt)
+                 max_iter=cfg.get("max_iter", 1000), precision=precision, format=fmt,
+                 cycle=cfg.get("cycle", "v"), cgc=cfg.get("cgc", "fixed"))
     b = mg.assemble_rhs(str(fx["rhs_kind"]))
     return mg, mg.solve(b)
 
@@ -45,6 +46,40 @@ def test_fp64_solve_matches_reference_solver(name, fmt):
     assert res["iters"] == int(fx["iters"])
     np.testing.assert_allclose(res["hist"], fx["hist"], rtol=1e-5)
     assert relerr(res["u"].cpu().numpy(), fx["u"]) <= 1e-10
+
+
+CYCLE_FIXTURES = ["ref_cycle_f_q1_2d_L6", "ref_cycle_w_q1_3d_L4", "ref_cgc_energy_q1_2d_L6",
+                  "ref_cgc_defect_f_q1_2d_L6", "ref_cycle_w_richardson_q1_2d_L5"]
+
+
+@pytest.mark.parametrize("name", CYCLE_FIXTURES)
+@pytest.mark.parametrize("fmt", ["sell", "stencil", "matfree"])
+def test_fw_cycles_and_adaptive_cgc_match_reference(name, fmt):
+    """F and W cycles, MinEnergy / MinDefect coarse-grid corrections (multigrid.hpp:1354-1519,
+    1898-1925) against the reference solver's own outputs"""
+    fx = load(name)
+    _, res = gpu_solve(fx, fmt)
+    assert res["status"] == "success"
+    assert res["iters"] == int(fx["iters"])
+    np.testing.assert_allclose(res["hist"], fx["hist"], rtol=1e-5)
+    assert relerr(res["u"].cpu().numpy(), fx["u"]) <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["ref_cycle_w_q1_3d_L4", "ref_cgc_defect_f_q1_2d_L6"])
+@pytest.mark.parametrize("precision", ["f32", "f16"])
+def test_fw_cycles_mixed_precision(name, precision):
+    """mixed forms of the F/W-cycle compositions: error against the FP64 oracle solution
+    (same composition, converged to 1e-12) within 1e-8"""
+    from oracle import pyoracle as po
+    fx = load(name)
+    cfg = fx["cfg"]
+    H = po.Hierarchy(int(fx["dim"]), int(fx["degree"]), int(fx["level"]), int(fx["level_min"]), fx.get("k"))
+    ref = H.solve(H.rhs(str(fx["rhs_kind"])), nu=cfg["nu"], omega_jac=cfg["omega_jac"], coarse=cfg["coarse"],
+                  tol=1e-12, cycle=cfg.get("cycle", "v"), cgc=cfg.get("cgc", "fixed"))
+    _, res = gpu_solve(fx, "matfree", precision=precision)
+    assert res["status"] == "success"
+    assert abs(res["iters"] - int(fx["iters"])) <= 1
+    assert relerr(res["u"].cpu().numpy(), ref["u"]) <= 1e-8
 
 
 @pytest.mark.parametrize("fmt", ["sell", "stencil"])
