@@ -15,9 +15,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HEADER = os.path.join(os.path.dirname(HERE), "include", "feat3_b200.h")
 
 (FB_OK, FB_ERR_INVALID, FB_ERR_CUDA, FB_ERR_ALLOC, FB_ERR_UNSUPPORTED, FB_ERR_NOT_READY, FB_ERR_TOO_LARGE,
- FB_ERR_TIMEOUT) = range(8)
+ FB_ERR_TIMEOUT, FB_ERR_IO, FB_ERR_FORMAT) = range(10)
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "allocation failed", 4: "unsupported", 5: "not ready",
-          6: "exceeds a fixed capacity", 7: "bounded wait in a kernel expired"}
+          6: "exceeds a fixed capacity", 7: "bounded wait in a kernel expired", 8: "file I/O error",
+          9: "contents do not match the file format"}
 
 
 class FeatError(RuntimeError):
@@ -101,9 +102,22 @@ _SIGS = {
     "fb_mg_adjoint_grad": [vp, vp, vp, vp, vp, C.POINTER(SolveInfo)],
     "fb_mg_element_grad": [vp, vp, vp, vp],
     "fb_mg_time_spmv": [vp, i32, i32, i32, i32, C.POINTER(dbl)],
+    # container file I/O
+    "fb_io_csr_read": [C.c_char_p, i32, C.POINTER(CsrHost)],
+    "fb_io_csr_write": [C.c_char_p, i32, C.POINTER(CsrHost), i32],
+    "fb_io_csr_serialised_size": [C.POINTER(CsrHost), C.POINTER(u64)],
+    "fb_io_csr_serialise": [C.POINTER(CsrHost), vp, u64],
+    "fb_io_csr_deserialise": [vp, u64, C.POINTER(CsrHost)],
+    "fb_io_csr_release": [C.POINTER(CsrHost)],
+    "fb_io_vector_read": [C.c_char_p, i32, C.POINTER(u64), C.POINTER(C.POINTER(dbl))],
+    "fb_io_vector_write": [C.c_char_p, i32, vp, u64],
+    "fb_io_vector_serialised_size": [u64, C.POINTER(u64)],
+    "fb_io_vector_serialise": [vp, u64, vp, u64],
+    "fb_io_vector_deserialise": [vp, u64, C.POINTER(u64), C.POINTER(C.POINTER(dbl))],
+    "fb_io_free": [vp],
     "fb_version": [],
 }
-_RESTYPE = {"fb_mg_destroy": None, "fb_solver_cfg_default": None, "fb_mg_num_dofs": u64,
+_RESTYPE = {"fb_mg_destroy": None, "fb_io_csr_release": None, "fb_io_free": None, "fb_solver_cfg_default": None, "fb_mg_num_dofs": u64,
             "fb_mg_nnz": u64, "fb_version": C.c_char_p}
 
 _lib = None

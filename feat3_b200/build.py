@@ -2,7 +2,7 @@
 
     python -m feat3_b200.build          # -> feat3_b200/libfeat3_b200.so
 
-nvcc compiles every ``csrc/*.cu`` for ``sm_100a`` and links one shared library with a
+nvcc compiles every ``csrc/*.cu`` for ``sm_100a`` (and the host-only ``csrc/*.cpp``) and links one shared library with a
 plain C ABI (``include/feat3_b200.h``). The CUDA runtime is linked statically, so the
 library only needs the driver at run time.
 """
@@ -23,7 +23,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompil
 
 
 def sources():
-    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")) + glob.glob(os.path.join(HERE, "csrc", "*.cpp")))
 
 
 def deps():

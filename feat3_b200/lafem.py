@@ -100,6 +100,16 @@ class DenseVector:
         self.t.copy_(x.t)
         return self
 
+    # DenseVector(FileMode, filename) / read_from / write_out (dense_vector.hpp:587-777)
+    @classmethod
+    def from_file(cls, mode, filename, dtype=torch.float64):
+        from . import fileio
+        return cls(torch.as_tensor(fileio.read_vector(mode, filename)).to(dtype).cuda())
+
+    def write_out(self, mode, filename):
+        from . import fileio
+        fileio.write_vector(mode, filename, self.t.double().cpu().numpy())
+
     def convert(self, x):
         """precision conversion (MemoryPool<Mem::CUDA>::convert)"""
         if self.dtype == x.dtype:
@@ -146,6 +156,20 @@ class SparseMatrixCSR:
         _lib.call(f"fb_diagonal_csr_{_sfx(self.dtype)}", _p(d.t), _p(self.val), _p(self.col_ind), _p(self.row_ptr),
                   self.rows, _stream())
         return d
+
+    # SparseMatrixCSR(FileMode, filename) / read_from / write_out (sparse_matrix_csr.hpp:1098-1343)
+    @classmethod
+    def from_file(cls, mode, filename, dtype=torch.float64):
+        from . import fileio
+        m = fileio.read_csr(mode, filename)
+        return cls(m.row_ptr, m.col_ind, m.val, columns=m.columns, dtype=dtype)
+
+    def write_out(self, mode, filename, symmetric=False):
+        from . import fileio
+        m = fileio.CsrFile(self.rows, self.columns, self.row_ptr.cpu().numpy().view(np.uint32).astype(np.uint64),
+                           self.col_ind.cpu().numpy().view(np.uint32).astype(np.uint64),
+                           self.val.double().cpu().numpy())
+        fileio.write_csr(mode, filename, m, symmetric=symmetric)
 
 
 class SparseMatrixELL:

@@ -1,7 +1,7 @@
 /*
  * feat3_b200 -- C-ABI of the B200 (sm_100a) geometric-multigrid Poisson path.
  *
- * Two layers:
+ * Three layers:
  *  1. Operator layer: one entry point per FEAT3 backend function of the LAFEM arch
  *     boundary for Mem::CUDA (kernel/lafem/arch/*.hpp). A FEAT3 build binds
  *     LAFEM::Arch::<Op><Mem::CUDA> onto these, so the reference's
@@ -10,6 +10,8 @@
  *     these kernels unchanged.
  *  2. Solver layer: a native multigrid driver (hierarchy, fused V-cycle, PCG/Richardson,
  *     mixed precision, adjoint) for callers that hand over a whole hierarchy.
+ *  3. Container file I/O: FEAT3's binary and text formats for matrices and vectors, so a
+ *     hierarchy written by a FEAT3 application can be loaded into the solver layer (host code).
  *
  * Conventions: all array pointers of the operator layer are DEVICE pointers; indices are
  * 32-bit unsigned (the reference's 64-bit Index arrays are narrowed once at upload);
@@ -286,6 +288,45 @@ FB_API int fb_mg_element_grad(fb_mg* mg, const double* u, const double* lambda, 
  * which: 0 = fused defect + Jacobi update (the smoother step), 1 = defect, 2 = PCG q = A p
  * with q.p; precision selects the value storage (FB_PREC_*). */
 FB_API int fb_mg_time_spmv(fb_mg* mg, int level, int which, int precision, int reps, double* ms_per_launch);
+
+/* ===================================================================================== */
+/* 3. Container file I/O in FEAT3's formats (host only, no device needed)                */
+/* ===================================================================================== */
+
+/* File modes: the values of LAFEM::FileMode (kernel/lafem/base.hpp:31-46). */
+#define FB_FILE_EXP 0      /* fm_exp: one value per line (vectors) */
+#define FB_FILE_DV 1       /* fm_dv: serialised DenseVector */
+#define FB_FILE_MTX 2      /* fm_mtx: MatrixMarket text */
+#define FB_FILE_CSR 4      /* fm_csr: serialised SparseMatrixCSR */
+#define FB_FILE_BINARY 12  /* fm_binary: the serialised form of the container type */
+#define FB_ERR_IO 8        /* a file could not be opened, read or written */
+#define FB_ERR_FORMAT 9    /* file or buffer contents do not match the requested format */
+
+/* Read a CSR matrix from `path` (FB_FILE_MTX general or symmetric, FB_FILE_CSR,
+ * FB_FILE_BINARY). The arrays of *out are allocated by the library; free them with
+ * fb_io_csr_release. The result can be handed to fb_mg_create_csr as is.
+ * Replaces SparseMatrixCSR::read_from (kernel/lafem/sparse_matrix_csr.hpp:1098-1246). */
+FB_API int fb_io_csr_read(const char* path, int mode, fb_csr_host* out);
+/* Write a CSR matrix (FB_FILE_MTX, FB_FILE_CSR, FB_FILE_BINARY); symmetric != 0 writes the
+ * lower triangle as "coordinate real symmetric" (FB_FILE_MTX only), byte for byte as
+ * SparseMatrixCSR::write_out (sparse_matrix_csr.hpp:1261-1343). */
+FB_API int fb_io_csr_write(const char* path, int mode, const fb_csr_host* m, int symmetric);
+/* In-memory serialisation in the fm_csr layout (SparseMatrixCSR::serialise/deserialise,
+ * sparse_matrix_csr.hpp:1066-1090; Container::_serialise, container.hpp:317-572). */
+FB_API int fb_io_csr_serialised_size(const fb_csr_host* m, uint64_t* size);
+FB_API int fb_io_csr_serialise(const fb_csr_host* m, void* buf, uint64_t capacity);
+FB_API int fb_io_csr_deserialise(const void* buf, uint64_t size, fb_csr_host* out);
+FB_API void fb_io_csr_release(fb_csr_host* m);
+
+/* Read / write a dense vector (FB_FILE_EXP, FB_FILE_MTX, FB_FILE_DV, FB_FILE_BINARY); *data
+ * is allocated by the library, free it with fb_io_free. Replaces DenseVector::read_from /
+ * write_out / serialise / deserialise (kernel/lafem/dense_vector.hpp:480-505, 587-777). */
+FB_API int fb_io_vector_read(const char* path, int mode, uint64_t* n, double** data);
+FB_API int fb_io_vector_write(const char* path, int mode, const double* data, uint64_t n);
+FB_API int fb_io_vector_serialised_size(uint64_t n, uint64_t* size);
+FB_API int fb_io_vector_serialise(const double* data, uint64_t n, void* buf, uint64_t capacity);
+FB_API int fb_io_vector_deserialise(const void* buf, uint64_t size, uint64_t* n, double** data);
+FB_API void fb_io_free(void* p);
 
 /* library version string */
 FB_API const char* fb_version(void);

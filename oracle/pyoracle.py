@@ -202,7 +202,7 @@ def _read_info(fn):
 
 def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", nu=4, omega_jac=0.5,
             omega_rich=1.0, omega_outer=1.0, coarse="direct", tol=1e-8, max_iter=1000, inner="f64",
-            target=None, dump_matrices=False, workdir=None, cycle="v", cgc="fixed"):
+            target=None, dump_matrices=False, workdir=None, cycle="v", cgc="fixed", feat_files=False):
     """Run the reference's own FP64/mixed MG solver; returns info and arrays in lattice order."""
     if not have_ref():
         raise FileNotFoundError(REF_BIN)
@@ -224,6 +224,8 @@ def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", n
         cmd += ["--target", tf]
     if dump_matrices:
         cmd += ["--dump-matrices"]
+    if feat_files:
+        cmd += ["--feat-files"]
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
     info = _read_info(out + ".info")
     lat = np.fromfile(out + ".lattice", dtype=np.uint64).astype(np.int64)

@@ -88,6 +88,7 @@ namespace RefDriver
     std::string target;            // adjoint: u_target in lexicographic DOF lattice order
     std::string out = "ref";
     bool dump_matrices = false;
+    bool feat_files = false;       // also write the hierarchy through the reference's own write_out
     bool quiet = false;
   };
 
@@ -410,6 +411,46 @@ namespace RefDriver
       write_f64(pre + ".val", va);
     }
 
+    // The hierarchy in the reference's own container file formats (SparseMatrixCSR::write_out,
+    // kernel/lafem/sparse_matrix_csr.hpp:1261-1343), plus the reference's parse of its own
+    // text files written back in binary form (read_from, sparse_matrix_csr.hpp:1098-1246),
+    // so both directions of the I/O layer can be checked against the reference.
+    void write_feat_files(const std::string& pre, const Level& lv, bool transfers) const
+    {
+      lv.matrix.write_out(LAFEM::FileMode::fm_csr, pre + ".A.csr");
+      lv.matrix.write_out(LAFEM::FileMode::fm_mtx, pre + ".A.mtx");
+      lv.matrix.write_out(LAFEM::FileMode::fm_mtx, pre + ".A.sym.mtx", true);
+      for(const char* nm : {".A.mtx", ".A.sym.mtx"})
+      {
+        MatrixType back;
+        back.read_from(LAFEM::FileMode::fm_mtx, pre + nm);
+        back.write_out(LAFEM::FileMode::fm_csr, pre + nm + ".csr");
+      }
+      MatrixType bin;
+      bin.read_from(LAFEM::FileMode::fm_binary, pre + ".A.csr");
+      bin.write_out(LAFEM::FileMode::fm_binary, pre + ".A.csr.csr");
+      if(transfers)
+      {
+        lv.transfer.get_mat_prol().write_out(LAFEM::FileMode::fm_csr, pre + ".P.csr");
+        lv.transfer.get_mat_prol().write_out(LAFEM::FileMode::fm_mtx, pre + ".P.mtx");
+        lv.transfer.get_mat_rest().write_out(LAFEM::FileMode::fm_csr, pre + ".R.csr");
+        lv.transfer.get_mat_rest().write_out(LAFEM::FileMode::fm_mtx, pre + ".R.mtx");
+      }
+    }
+
+    // DenseVector::write_out / read_from (kernel/lafem/dense_vector.hpp:587-777)
+    static void write_feat_vector(const std::string& pre, const VectorType& v)
+    {
+      v.write_out(LAFEM::FileMode::fm_dv, pre + ".dv");
+      v.write_out(LAFEM::FileMode::fm_exp, pre + ".exp");
+      v.write_out(LAFEM::FileMode::fm_mtx, pre + ".vmtx");
+      VectorType a, b;
+      a.read_from(LAFEM::FileMode::fm_exp, pre + ".exp");
+      a.write_out(LAFEM::FileMode::fm_dv, pre + ".exp.dv");
+      b.read_from(LAFEM::FileMode::fm_mtx, pre + ".vmtx");
+      b.write_out(LAFEM::FileMode::fm_dv, pre + ".vmtx.dv");
+    }
+
     int run()
     {
       info.open(cfg.out + ".info");
@@ -553,7 +594,11 @@ namespace RefDriver
             dump_csr(pre + ".P", lv.transfer.get_mat_prol());
             dump_csr(pre + ".R", lv.transfer.get_mat_rest());
           }
+          if(cfg.feat_files)
+            write_feat_files(pre, lv, i + 1 < levels.size());
         }
+        if(cfg.feat_files)
+          write_feat_vector(cfg.out + ".rhs", vec_rhs);
       }
 
       // ---- solve
@@ -568,6 +613,8 @@ namespace RefDriver
         solve_mixed(vec_sol, vec_rhs, hist, iters, status, solve_time);
 
       write_f64(cfg.out + ".u", std::vector<double>(vec_sol.elements(), vec_sol.elements() + vec_sol.size()));
+      if(cfg.feat_files)
+        vec_sol.write_out(LAFEM::FileMode::fm_dv, cfg.out + ".u.dv");
 
       info << "n_dofs " << top.space.get_num_dofs() << "\n";
       info << "n_cells " << top.mesh.get_num_elements() << "\n";
@@ -836,6 +883,7 @@ int main(int argc, char** argv)
     else if(a == "--target") cfg.target = next();
     else if(a == "--out") cfg.out = next();
     else if(a == "--dump-matrices") cfg.dump_matrices = true;
+    else if(a == "--feat-files") cfg.dump_matrices = cfg.feat_files = true;
     else if(a == "--quiet") cfg.quiet = true;
     else { std::cerr << "unknown option " << a << std::endl; return 2; }
   }

@@ -7,11 +7,13 @@ lattice numbering through the DOF coordinates, as compressed .npz files:
 
     python tests/golden/gen_golden.py          # needs oracle/_ref/feat_ref
     python tests/golden/gen_golden.py --cycles # only the F/W-cycle and adaptive-CGC fixtures
+    python tests/golden/gen_golden.py --files  # only the container-file fixtures (feat_files_q1_2d_L3/)
 
 Inputs that are random (coefficient fields, target noise) are drawn here with numpy's
 seeded generator and stored in the fixture next to the outputs.
 """
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -66,11 +68,34 @@ def cycles():
         omega_rich=1.0, coarse="smoother", tol=1e-8, cycle="w")
 
 
+def feat_files():
+    """The hierarchy of the 2D Q1 level-3 case (levels 3..1) as written by the reference's own
+    SparseMatrixCSR/DenseVector::write_out (sparse_matrix_csr.hpp:1261-1343, dense_vector.hpp:
+    721-777), and the reference's own parse of its text files written back in binary (*.mtx.csr,
+    *.exp.dv, *.vmtx.dv; read_from, sparse_matrix_csr.hpp:1098-1246, dense_vector.hpp:587-712)."""
+    R = po.run_ref(2, 1, 3, 1, rhs="sine", solver="pcg", nu=2, coarse="direct", tol=1e-8, feat_files=True)
+    pre = R["prefix"]
+    out = os.path.join(HERE, "feat_files_q1_2d_L3")
+    os.makedirs(out, exist_ok=True)
+    names = [f"L{l}.A.csr" for l in (1, 2, 3)] + [f"L{l}.{m}.csr" for l in (2, 3) for m in "PR"]
+    names += ["L3.A.mtx", "L3.A.sym.mtx", "L3.A.mtx.csr", "L3.A.sym.mtx.csr", "L3.P.mtx", "L3.R.mtx"]
+    names += ["rhs.dv", "rhs.exp", "rhs.vmtx", "rhs.exp.dv", "rhs.vmtx.dv", "u.dv"]
+    total = 0
+    for nm in names:
+        shutil.copyfile(f"{pre}.{nm}", os.path.join(out, nm))
+        total += os.path.getsize(os.path.join(out, nm))
+    with open(os.path.join(out, "iters.txt"), "w") as f:
+        f.write(f"{R['info']['iters']}\n")
+    print(f"{out}: {len(names)} files, {total / 1024:.1f} KiB")
+
+
 def main():
     if not po.have_ref():
         sys.exit("oracle/_ref/feat_ref is missing: build it with `make -C oracle ref` first")
     if "--cycles" in sys.argv:
         return cycles()
+    if "--files" in sys.argv:
+        return feat_files()
     rng = np.random.default_rng(20261203)
     # applications/poisson_dirichlet.cpp composition, level 5, the reference's pin (4 +- 1 iterations,
     # applications/CMakeLists.txt:100-108)
@@ -117,6 +142,8 @@ def main():
         arrays[f"L{l}_filter"] = np.fromfile(f"{pre}.L{l}.filter", dtype=np.uint64)
         arrays[f"L{l}_lattice"] = np.fromfile(f"{pre}.L{l}.lattice", dtype=np.uint64)
     save("ref_matrices_q1_2d_L3", **arrays)
+    cycles()
+    feat_files()
 
 
 if __name__ == "__main__":
