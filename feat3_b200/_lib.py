@@ -32,7 +32,7 @@ vp, u64, u32, i32, dbl, flt = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_d
 
 class StructuredDesc(C.Structure):
     _fields_ = [("dim", i32), ("degree", i32), ("level", i32), ("level_min", i32),
-                ("k", vp), ("k_on_device", i32), ("sell_sigma", i32)]
+                ("k", vp), ("k_on_device", i32), ("sell_sigma", i32), ("numbering", i32)]
 
 
 class CsrHost(C.Structure):
@@ -86,6 +86,7 @@ _SIGS = {
     "fb_set_f32": [vp, flt, u64, vp],
     # solver layer
     "fb_mg_create_structured": [C.POINTER(vp), C.POINTER(StructuredDesc)],
+    "fb_feat_numbering": [i32, i32, i32, vp, vp, vp],
     "fb_mg_create_csr": [C.POINTER(vp), i32, vp, vp, vp, vp, vp, i32],
     "fb_mg_destroy": [vp],
     "fb_solver_cfg_default": [C.POINTER(SolverCfg)],

@@ -20,6 +20,7 @@
 // transposes (tutorial_05_multigrid.cpp:302).
 #include "fb_mg_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -536,6 +537,7 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
     const uint64_t row_max = d->dim == 3 ? (d->degree == 1 ? 27 : 125) : (d->degree == 1 ? 9 : 25);
     if (n * row_max >= 0xffffffffull) return FB_ERR_INVALID;  // 32-bit slot addressing
     if (d->degree == 2 && (d->level_min < 1)) return FB_ERR_INVALID;  // Q2 transfer needs >= 2 cells
+    if (d->numbering != FB_NUMBERING_LATTICE && d->numbering != FB_NUMBERING_FEAT) return FB_ERR_INVALID;
   }
   fb_mg* m = new fb_mg();
   int st = common_init(m);
@@ -558,6 +560,15 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
   do {
     st = dupload(m, &m->kref, m->kref_h.data(), m->kref_h.size());
     if (st != FB_OK) break;
+    if (d->numbering == FB_NUMBERING_FEAT) {
+      // the finest level's DOF and cell numbering of FEAT's refined unit square / cube
+      const Geom g = geom_of(m, d->level);
+      const uint64_t n = uint64_t(g.M1) * g.M1 * (m->dim == 3 ? g.M1 : 1);
+      const uint64_t ne = uint64_t(g.N) * g.N * (m->dim == 3 ? g.N : 1);
+      if ((st = dalloc(m, &m->feat_dof, n)) != FB_OK || (st = dalloc(m, &m->feat_cell, ne)) != FB_OK) break;
+      st = feat_numbering(m->dim, m->degree, d->level, m->feat_dof, m->feat_cell, m->stream);
+      if (st != FB_OK) break;
+    }
     // coefficients, finest first
     for (int i = 0; i < nl && st == FB_OK; ++i) {
       const int lvl = d->level - i;
@@ -571,9 +582,13 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
         if (st != FB_OK) break;
         if (i == 0) {
           // stream-ordered copy; a device-side k must be complete before this call (the caller's stream)
-          if (cudaMemcpyAsync(L.k, d->k, sizeof(double) * L.ne, d->k_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+          double* dst = L.k;
+          if (m->feat_cell && (st = dalloc(m, &m->pcell, L.ne)) != FB_OK) break;
+          if (m->feat_cell) dst = m->pcell;  // FEAT cell order: staged, then permuted
+          if (cudaMemcpyAsync(dst, d->k, sizeof(double) * L.ne, d->k_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                               m->stream) != cudaSuccess ||
-              cudaStreamSynchronize(m->stream) != cudaSuccess) st = FB_ERR_CUDA;
+              cudaStreamSynchronize(m->stream) != cudaSuccess) { st = FB_ERR_CUDA; break; }
+          if (m->feat_cell) st = perm_to_lattice(m, L.k, m->pcell, m->feat_cell, L.ne);
         } else {
           k_coarsen_k<<<grid_for(L.ne, 256), 256, 0, m->stream>>>(m->dim, g.N, m->L[i - 1].k, L.k);
           if (cudaGetLastError() != cudaSuccess) st = FB_ERR_CUDA;
@@ -664,8 +679,15 @@ int fb_mg_assemble_rhs(fb_mg* m, int kind, double* rhs) {
   if (!m->structured) return FB_ERR_UNSUPPORTED;
   FB_CUDA(cudaSetDevice(m->device));
   const Geom g = geom_of(m, m->level);
-  k_rhs<<<grid_for(m->L[0].n, 128), 128, 0, m->stream>>>(g, m->L[0].n, kind, m->L[0].mask, rhs);
+  const uint32_t n = m->L[0].n;
+  double* out = rhs;
+  if (m->feat_dof) {
+    if (!m->pv1) FB_TRY(dalloc(m, &m->pv1, n));
+    out = m->pv1;
+  }
+  k_rhs<<<grid_for(n, 128), 128, 0, m->stream>>>(g, n, kind, m->L[0].mask, out);
   FB_CHECK_LAUNCH();
+  if (m->feat_dof) FB_TRY(perm_from_lattice(m, rhs, out, m->feat_dof, n));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   return FB_OK;
 }
@@ -687,27 +709,73 @@ int fb_mg_export_csr(fb_mg* m, int l, uint64_t* rp, uint32_t* col, double* val) 
   }
   std::vector<uint32_t> slot_of(S.rows);
   for (uint32_t sr = 0; sr < S.rows; ++sr) slot_of[perm.empty() ? sr : perm[sr]] = sr;
+  // finest level in FEAT numbering: row f is lattice row feat[f], columns renumbered and sorted
+  std::vector<uint32_t> feat, lat_to_feat;
+  if (m->feat_dof && l == 0) {
+    feat.resize(S.rows);
+    lat_to_feat.resize(S.rows);
+    FB_CUDA(cudaMemcpy(feat.data(), m->feat_dof, sizeof(uint32_t) * S.rows, cudaMemcpyDeviceToHost));
+    for (uint32_t f = 0; f < S.rows; ++f) lat_to_feat[feat[f]] = f;
+  }
   rp[0] = 0;
-  for (uint32_t r = 0; r < S.rows; ++r) rp[r + 1] = rp[r] + rl[r];
+  for (uint32_t r = 0; r < S.rows; ++r) rp[r + 1] = rp[r] + rl[feat.empty() ? r : feat[r]];
+  std::vector<std::pair<uint32_t, double>> row;
   for (uint32_t r = 0; r < S.rows; ++r) {
-    const uint32_t sr = slot_of[r], c = sr / 32, t = sr % 32;
-    for (uint32_t j = 0; j < rl[r]; ++j) {
-      col[rp[r] + j] = cc[cs[c] + uint64_t(j) * 32 + t];
-      val[rp[r] + j] = vv[cs[c] + uint64_t(j) * 32 + t];
+    const uint32_t lr = feat.empty() ? r : feat[r];
+    const uint32_t sr = slot_of[lr], c = sr / 32, t = sr % 32;
+    row.clear();
+    for (uint32_t j = 0; j < rl[lr]; ++j) {
+      const uint32_t cl = cc[cs[c] + uint64_t(j) * 32 + t];
+      row.emplace_back(feat.empty() ? cl : lat_to_feat[cl], vv[cs[c] + uint64_t(j) * 32 + t]);
+    }
+    if (!feat.empty()) std::sort(row.begin(), row.end(), [](const std::pair<uint32_t, double>& a, const std::pair<uint32_t, double>& b) { return a.first < b.first; });
+    for (uint32_t j = 0; j < rl[lr]; ++j) {
+      col[rp[r] + j] = row[j].first;
+      val[rp[r] + j] = row[j].second;
     }
   }
   return FB_OK;
 }
 
+}  // extern "C"
+
+namespace fb {
+// element gradient with u and lam in lattice order; grad in the C-ABI's cell order
+static int element_grad_lattice(fb_mg* m, const double* u, const double* lam, double* grad) {
+  const Geom g = geom_of(m, m->level);
+  const uint64_t ne = m->L[0].ne;
+  double* out = grad;
+  if (m->feat_cell) {
+    if (!m->pcell) FB_TRY(dalloc(m, &m->pcell, ne));
+    out = m->pcell;
+  }
+  k_elem_grad<<<grid_for(ne, 128), 128, 0, m->stream>>>(g, ne, u, lam, m->kref, elem_scale(m->dim, m->level), out);
+  FB_CHECK_LAUNCH();
+  if (m->feat_cell) FB_TRY(perm_from_lattice(m, grad, out, m->feat_cell, ne));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  return FB_OK;
+}
+
+static int ensure_stage(fb_mg* m) {
+  const uint32_t n = m->L[0].n;
+  if (!m->pv1) FB_TRY(dalloc(m, &m->pv1, n));
+  if (!m->pv2) FB_TRY(dalloc(m, &m->pv2, n));
+  if (!m->pv3) FB_TRY(dalloc(m, &m->pv3, n));
+  return FB_OK;
+}
+}  // namespace fb
+
+extern "C" {
+
 int fb_mg_element_grad(fb_mg* m, const double* u, const double* lam, double* grad) {
   if (!m || !u || !lam || !grad) return FB_ERR_INVALID;
   if (!m->structured) return FB_ERR_UNSUPPORTED;
   FB_CUDA(cudaSetDevice(m->device));
-  const Geom g = geom_of(m, m->level);
-  k_elem_grad<<<grid_for(m->L[0].ne, 128), 128, 0, m->stream>>>(g, m->L[0].ne, u, lam, m->kref, elem_scale(m->dim, m->level), grad);
-  FB_CHECK_LAUNCH();
-  FB_CUDA(cudaStreamSynchronize(m->stream));
-  return FB_OK;
+  FB_TRY(ensure_stage(m));
+  const double *ul, *laml;
+  FB_TRY(in_lattice(m, u, m->pv1, &ul));
+  FB_TRY(in_lattice(m, lam, m->pv2, &laml));
+  return element_grad_lattice(m, ul, laml, grad);
 }
 
 int fb_mg_adjoint_grad(fb_mg* m, const double* u, const double* ut, double* lam, double* grad, fb_solve_info* info) {
@@ -717,12 +785,19 @@ int fb_mg_adjoint_grad(fb_mg* m, const double* u, const double* ut, double* lam,
   FB_CUDA(cudaSetDevice(m->device));
   const uint32_t n = m->L[0].n;
   if (!m->adj) FB_TRY(dalloc(m, &m->adj, n));
-  k_adj_rhs<<<ew_grid(n), 256, 0, m->stream>>>(m->adj, u, ut, m->L[0].mask, n);
+  FB_TRY(ensure_stage(m));
+  // everything below in lattice order; lam and grad leave in the C-ABI's numbering
+  const double *ul, *utl;
+  FB_TRY(in_lattice(m, u, m->pv1, &ul));
+  FB_TRY(in_lattice(m, ut, m->pv2, &utl));
+  double* laml = m->feat_dof ? m->pv3 : lam;
+  k_adj_rhs<<<ew_grid(n), 256, 0, m->stream>>>(m->adj, ul, utl, m->L[0].mask, n);
   FB_CHECK_LAUNCH();
-  FB_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * n, m->stream));
+  FB_CUDA(cudaMemsetAsync(laml, 0, sizeof(double) * n, m->stream));
   // A is symmetric and R = P^T, so the transposed MG-PCG is the configured solver itself
-  FB_TRY(solve_dev(m, m->adj, lam, nullptr, info));
-  return fb_mg_element_grad(m, u, lam, grad);
+  FB_TRY(solve_dev(m, m->adj, laml, nullptr, info, false));
+  if (m->feat_dof) FB_TRY(perm_from_lattice(m, lam, laml, m->feat_dof, n));
+  return element_grad_lattice(m, ul, laml, grad);
 }
 
 }  // extern "C"

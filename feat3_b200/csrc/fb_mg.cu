@@ -1444,15 +1444,21 @@ static int check_kernel_waits(fb_mg* m) {
 }
 
 // ------------------------------------------------------------------ solve
-int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info) {
+int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info, bool feat_io) {
   if (!m->configured) return FB_ERR_NOT_READY;
   FB_TRY(ensure_vectors(m, m->cfg.precision));
   const uint32_t n = m->L[0].n;
   cudaStream_t s = m->stream;
+  const uint32_t* perm = feat_io ? m->feat_dof : nullptr;
   m->launches = 0;
   FB_CUDA(cudaEventRecord(m->ev0, s));
-  FB_CUDA(cudaMemcpyAsync(m->bb, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  FB_CUDA(cudaMemcpyAsync(m->xb, sol, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (perm) {
+    FB_TRY(perm_to_lattice(m, m->bb, rhs, perm, n));
+    FB_TRY(perm_to_lattice(m, m->xb, sol, perm, n));
+  } else {
+    FB_CUDA(cudaMemcpyAsync(m->bb, rhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    FB_CUDA(cudaMemcpyAsync(m->xb, sol, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  }
   // correct(): r = filter_def(b - A x) (pcg.hpp:158-172, richardson.hpp:174-185)
   FB_TRY(outer_defect(m));
   if (m->cfg.outer == FB_OUTER_PCG) {
@@ -1487,7 +1493,8 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
     if (hist) hist[it] = d;
     status = st.analyse(it, d);
   }
-  FB_CUDA(cudaMemcpyAsync(sol, m->xb, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (perm) FB_TRY(perm_from_lattice(m, sol, m->xb, perm, n));
+  else FB_CUDA(cudaMemcpyAsync(sol, m->xb, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   FB_CUDA(cudaEventRecord(m->ev1, s));
   FB_CUDA(cudaEventSynchronize(m->ev1));
   FB_TRY(check_kernel_waits(m));
@@ -1651,7 +1658,8 @@ int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
   FB_TRY(ensure_vectors(m, m->cfg.precision));
   const uint32_t n = m->L[0].n;
   cudaStream_t s = m->stream;
-  FB_CUDA(cudaMemcpyAsync(m->r, def, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (m->feat_dof) FB_TRY(perm_to_lattice(m, m->r, def, m->feat_dof, n));
+  else FB_CUDA(cudaMemcpyAsync(m->r, def, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
   k_dot_rz<double><<<occupancy_grid((const void*)k_dot_rz<double>, n / 32 + 1), 256, 0, s>>>(m->r, m->r, n, m->ws, m->counter, &m->sc->rr);
   FB_CHECK_LAUNCH();
   const void* z = nullptr;
@@ -1660,8 +1668,14 @@ int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
     FB_CHECK_LAUNCH();
   }
   FB_TRY(precond(m, &z));
-  if (m->cfg.precision == FB_PREC_F64) FB_CUDA(cudaMemcpyAsync(cor, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-  else { k_cvt<double, float><<<ew_grid(n), 256, 0, s>>>(cor, (const float*)z, n); FB_CHECK_LAUNCH(); }
+  double* out = cor;
+  if (m->feat_dof) {
+    if (!m->pv1) FB_TRY(dalloc(m, &m->pv1, n));
+    out = m->pv1;
+  }
+  if (m->cfg.precision == FB_PREC_F64) FB_CUDA(cudaMemcpyAsync(out, z, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  else { k_cvt<double, float><<<ew_grid(n), 256, 0, s>>>(out, (const float*)z, n); FB_CHECK_LAUNCH(); }
+  if (m->feat_dof) FB_TRY(perm_from_lattice(m, cor, out, m->feat_dof, n));
   FB_CUDA(cudaStreamSynchronize(s));
   return FB_OK;
 }

@@ -134,6 +134,13 @@ struct fb_mg {
   double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)                   // finest-level first smoothing step already formed (fused)
   double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
   double* adj = nullptr;                 // adjoint right-hand side
+  // FEAT numbering at the C-ABI (structured hierarchies created with FB_NUMBERING_FEAT):
+  // feat_dof[f] = lattice index of FEAT DOF f on the finest level, feat_cell[c] = lattice index
+  // of FEAT cell c; vectors cross the C-ABI in FEAT order and are permuted on the device
+  uint32_t* feat_dof = nullptr;
+  uint32_t* feat_cell = nullptr;
+  double *pv1 = nullptr, *pv2 = nullptr, *pv3 = nullptr;  // lattice-order staging (n each)
+  double* pcell = nullptr;                                 // lattice-order staging (cells)
 };
 
 namespace fb {
@@ -171,6 +178,13 @@ int upload_coarse_csr(fb_mg* m, const HostCsr& A);
 int upload_sell(fb_mg* m, DevSell& S, const HostCsr& A, int sigma);
 int upload_csr(fb_mg* m, DevCsr& D, const HostCsr& A);
 int upload_filter(fb_mg* m, Level& L, const std::vector<uint32_t>& f);
-int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info);
+// feat_io: rhs and sol are in the C-ABI's numbering (FEAT order when m->feat_dof is set)
+int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_info* info, bool feat_io = true);
 unsigned ew_grid(uint64_t n);
+int feat_numbering(int dim, int degree, int level, uint32_t* dof_lex, uint32_t* cell_lex, cudaStream_t s);
+// dst[perm[i]] = src[i] (FEAT order -> lattice order) and dst[i] = src[perm[i]] (back)
+int perm_to_lattice(fb_mg* m, double* dst, const double* src, const uint32_t* perm, uint64_t n);
+int perm_from_lattice(fb_mg* m, double* dst, const double* src, const uint32_t* perm, uint64_t n);
+// a finest-level vector of the C-ABI in lattice order: src itself, or src permuted into `stage`
+int in_lattice(fb_mg* m, const double* src, double* stage, const double** out);
 }  // namespace fb

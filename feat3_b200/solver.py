@@ -23,6 +23,21 @@ PRECISION = {"f64": 0, "f32": 1, "f16": 2}
 FORMAT = {"sell": 0, "stencil": 1, "matfree": 2}
 CYCLE = {"v": 0, "f": 1, "w": 2}
 CGC = {"fixed": 0, "energy": 1, "defect": 2}
+NUMBERING = {"lattice": 0, "feat": 1}
+
+
+def feat_numbering(dim, degree, level, device="cuda"):
+    """(dof_lex, cell_lex) as int64 CUDA tensors: the lexicographic lattice index of each FEAT3
+    DOF / cell of the unit square or cube refined `level` times (fb_feat_numbering)"""
+    n = (degree * (1 << level) + 1) ** dim
+    ne = (1 << level) ** dim
+    dofs = torch.empty(n, dtype=torch.int32, device=device)
+    cells = torch.empty(ne, dtype=torch.int32, device=device)
+    _lib.call("fb_feat_numbering", dim, degree, level, dofs.data_ptr(), cells.data_ptr(),
+              torch.cuda.current_stream().cuda_stream)
+    torch.cuda.current_stream().synchronize()
+    mask = (1 << 32) - 1
+    return dofs.to(torch.int64) & mask, cells.to(torch.int64) & mask
 RHS = {"sine": 0, "one": 1, "expbubble": 2}
 
 
@@ -42,10 +57,15 @@ class MultiGrid:
 
     # ---------------------------------------------------------------- construction
     @classmethod
-    def structured(cls, dim, degree, level, level_min=1, k=None, sell_sigma=1):
+    def structured(cls, dim, degree, level, level_min=1, k=None, sell_sigma=1, numbering="lattice"):
+        """Structured unit-square/cube hierarchy assembled on the device. numbering="feat" makes
+        every finest-level vector (rhs, solution, V-cycle, adjoint) and the coefficient / gradient
+        per cell use FEAT3's numbering of the refined unit cube instead of the lexicographic lattice."""
         lib = _lib.load()
         karr = None
-        desc = _lib.StructuredDesc(dim, degree, level, level_min, None, 0, sell_sigma)
+        if numbering not in NUMBERING:
+            raise ValueError(f"numbering must be one of {sorted(NUMBERING)}")
+        desc = _lib.StructuredDesc(dim, degree, level, level_min, None, 0, sell_sigma, NUMBERING[numbering])
         if k is not None:
             if isinstance(k, torch.Tensor) and k.is_cuda:
                 karr = k.contiguous().to(torch.float64)
@@ -58,6 +78,7 @@ class MultiGrid:
         _lib.check("fb_mg_create_structured", lib.fb_mg_create_structured(C.byref(h), C.byref(desc)))
         mg = cls(h, True)
         mg.dim, mg.degree, mg.level, mg.level_min = dim, degree, level, level_min
+        mg.numbering = numbering
         return mg
 
     @classmethod

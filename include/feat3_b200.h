@@ -157,8 +157,22 @@ typedef struct fb_structured_desc {
   const double* k;    /* per-element coefficient on the finest level or NULL */
   int k_on_device;    /* 1 if k is a device pointer */
   int sell_sigma;     /* SELL-C-sigma sorting window for the level matrices; 1 = no sorting */
+  int numbering;      /* FB_NUMBERING_LATTICE [0] or FB_NUMBERING_FEAT: the order of the finest
+                         level's DOFs and cells in every vector the solver layer takes or returns */
 } fb_structured_desc;
+#define FB_NUMBERING_LATTICE 0  /* lexicographic lattice, x fastest */
+#define FB_NUMBERING_FEAT 1     /* FEAT3's numbering of the refined unit square / cube */
 FB_API int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* desc);
+
+/* FEAT3's numbering of the unit square (dim 2) or cube (dim 3) refined `level` times by
+ * RefinedUnitCubeFactory / StandardRefinery (kernel/geometry/common_factories.hpp:71-235,
+ * conformal_mesh.hpp:439-528; the Q1/Q2 DOFs by DofMappingUniform, kernel/space/
+ * dof_mapping_common.hpp:255-330), computed on the device without building the mesh:
+ * dof_lex[f] = lexicographic lattice index of FEAT DOF f ((degree*2^level+1)^dim entries),
+ * cell_lex[c] = lexicographic index of FEAT cell c (2^(dim*level) entries). Device pointers;
+ * either may be NULL. Asynchronous on `stream`. */
+FB_API int fb_feat_numbering(int dim, int degree, int level, uint32_t* dof_lex, uint32_t* cell_lex,
+                             fb_stream_t stream);
 
 /* Hierarchy from caller-supplied CSR matrices (e.g. assembled by FEAT3 on the host in its
  * own numbering): level 0 = finest. Host pointers; copied to the device. P[l] maps level

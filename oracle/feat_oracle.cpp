@@ -9,6 +9,7 @@
 #include <limits>
 #include <memory>
 #include <type_traits>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -825,3 +826,171 @@ void or_csr_apply(double* r, double a, const double* x, double b, const double* 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// FEAT3 mesh numbering of the refined unit square / cube.
+//
+// Restates the standard refinement of conformal hypercube meshes:
+//  * new vertices: the old vertices, then one per edge, quad and hexa (in entity order) at its
+//    centre (StandardVertexRefiner, intern/standard_vertex_refiner.hpp:65-110, wrapper :195-253);
+//  * new entities of each dimension: the children of edges, then of quads, then of hexas, each
+//    parent's children consecutive (IndexRefineShapeWrapper, intern/standard_index_refiner.hpp:
+//    2762-2840), with the children's vertex lists of StandardIndexRefiner<Hypercube<d>,c,0>
+//    (:1346-1402, 1414-1497, 1505-1602, 1723-1811, 1819-2003, 2011-2174);
+//  * the unit cube: vertex i at the bits of i, sub-entities by FaceIndexMapping (face_index_
+//    mapping.hpp:119-183, common_factories.hpp:71-235);
+//  * DOFs of Lagrange1/Lagrange2: vertices, then edges, quads, hexas, one DOF per entity
+//    (DofMappingUniform, kernel/space/dof_mapping_common.hpp:255-330).
+// A child's vertex that the reference takes from the parent's edges-at-cell / quads-at-cell
+// sets (the vertex born from local edge or face k) is found here by its coordinates: the
+// centre of the parent's local edge or face k, as FaceIndexMapping numbers them.
+namespace {
+namespace numbering {
+const int kEdge2[4][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}};
+const int kEdge3[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+const int kFace3[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 4, 5}, {2, 3, 6, 7}, {0, 2, 4, 6}, {1, 3, 5, 7}};
+// local points of a parent: 'v' vertex k, 'e' centre of local edge k, 'q' centre of local
+// face k (hexa), 'x' the parent's centre
+struct Pt { char t; int k; };
+const Pt kQuadEdges[4][2] = {{{'e', 0}, {'x', 0}}, {{'x', 0}, {'e', 1}}, {{'e', 2}, {'x', 0}}, {{'x', 0}, {'e', 3}}};
+const Pt kQuadQuads[4][4] = {{{'v', 0}, {'e', 0}, {'e', 2}, {'x', 0}}, {{'e', 0}, {'v', 1}, {'x', 0}, {'e', 3}},
+                             {{'e', 2}, {'x', 0}, {'v', 2}, {'e', 1}}, {{'x', 0}, {'e', 3}, {'e', 1}, {'v', 3}}};
+const Pt kHexaEdges[6][2] = {{{'q', 0}, {'x', 0}}, {{'x', 0}, {'q', 1}}, {{'q', 2}, {'x', 0}},
+                             {{'x', 0}, {'q', 3}}, {{'q', 4}, {'x', 0}}, {{'x', 0}, {'q', 5}}};
+const Pt kHexaQuads[12][4] = {
+    {{'e', 0}, {'q', 0}, {'q', 2}, {'x', 0}}, {{'q', 0}, {'e', 1}, {'x', 0}, {'q', 3}},
+    {{'q', 2}, {'x', 0}, {'e', 2}, {'q', 1}}, {{'x', 0}, {'q', 3}, {'q', 1}, {'e', 3}},
+    {{'e', 4}, {'q', 0}, {'q', 4}, {'x', 0}}, {{'q', 0}, {'e', 5}, {'x', 0}, {'q', 5}},
+    {{'q', 4}, {'x', 0}, {'e', 6}, {'q', 1}}, {{'x', 0}, {'q', 5}, {'q', 1}, {'e', 7}},
+    {{'e', 8}, {'q', 2}, {'q', 4}, {'x', 0}}, {{'q', 2}, {'e', 9}, {'x', 0}, {'q', 5}},
+    {{'q', 4}, {'x', 0}, {'e', 10}, {'q', 3}}, {{'x', 0}, {'q', 5}, {'q', 3}, {'e', 11}}};
+const Pt kHexaHexas[8][8] = {
+    {{'v', 0}, {'e', 0}, {'e', 4}, {'q', 0}, {'e', 8}, {'q', 2}, {'q', 4}, {'x', 0}},
+    {{'e', 0}, {'v', 1}, {'q', 0}, {'e', 5}, {'q', 2}, {'e', 9}, {'x', 0}, {'q', 5}},
+    {{'e', 4}, {'q', 0}, {'v', 2}, {'e', 1}, {'q', 4}, {'x', 0}, {'e', 10}, {'q', 3}},
+    {{'q', 0}, {'e', 5}, {'e', 1}, {'v', 3}, {'x', 0}, {'q', 5}, {'q', 3}, {'e', 11}},
+    {{'e', 8}, {'q', 2}, {'q', 4}, {'x', 0}, {'v', 4}, {'e', 2}, {'e', 6}, {'q', 1}},
+    {{'q', 2}, {'e', 9}, {'x', 0}, {'q', 5}, {'e', 2}, {'v', 5}, {'q', 1}, {'e', 7}},
+    {{'q', 4}, {'x', 0}, {'e', 10}, {'q', 3}, {'e', 6}, {'q', 1}, {'v', 6}, {'e', 3}},
+    {{'x', 0}, {'q', 5}, {'q', 3}, {'e', 11}, {'q', 1}, {'e', 7}, {'e', 3}, {'v', 7}}};
+
+struct C3 { int64_t c[3]; };
+
+struct Mesh {
+  int dim = 2;
+  std::vector<C3> vtx;                         // integer coordinates (resolution R)
+  std::vector<std::vector<uint32_t>> ent[4];   // ent[d][i] = vertex list of entity i of dim d (d >= 1)
+};
+
+C3 centre(const Mesh& m, const std::vector<uint32_t>& vs, const int* loc, int n) {
+  C3 r{{0, 0, 0}};
+  for (int i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) r.c[a] += m.vtx[vs[loc[i]]].c[a];
+  for (int a = 0; a < 3; ++a) r.c[a] /= n;
+  return r;
+}
+
+C3 point(const Mesh& m, const std::vector<uint32_t>& vs, int pdim, Pt p) {
+  static const int all[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  switch (p.t) {
+    case 'v': return m.vtx[vs[p.k]];
+    case 'e': return centre(m, vs, pdim == 2 ? kEdge2[p.k] : kEdge3[p.k], 2);
+    case 'q': return centre(m, vs, kFace3[p.k], 4);
+    default: return centre(m, vs, all, 1 << pdim);
+  }
+}
+
+int64_t key(const C3& c, int64_t R) { return c.c[0] + (R + 1) * (c.c[1] + (R + 1) * c.c[2]); }
+
+Mesh unit_cube(int dim, int64_t R) {
+  Mesh m;
+  m.dim = dim;
+  for (int i = 0; i < (1 << dim); ++i) {
+    C3 c{{0, 0, 0}};
+    for (int a = 0; a < dim; ++a) c.c[a] = ((i >> a) & 1) * R;
+    m.vtx.push_back(c);
+  }
+  if (dim == 2) {
+    for (auto& e : kEdge2) m.ent[1].push_back({uint32_t(e[0]), uint32_t(e[1])});
+    m.ent[2].push_back({0, 1, 2, 3});
+  } else {
+    for (auto& e : kEdge3) m.ent[1].push_back({uint32_t(e[0]), uint32_t(e[1])});
+    for (auto& f : kFace3) m.ent[2].push_back({uint32_t(f[0]), uint32_t(f[1]), uint32_t(f[2]), uint32_t(f[3])});
+    m.ent[3].push_back({0, 1, 2, 3, 4, 5, 6, 7});
+  }
+  return m;
+}
+
+Mesh refine(const Mesh& m, int64_t R) {
+  Mesh f;
+  f.dim = m.dim;
+  f.vtx = m.vtx;
+  static const int all[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+  for (int d = 1; d <= m.dim; ++d)
+    for (auto& vs : m.ent[d]) f.vtx.push_back(centre(m, vs, all, 1 << d));
+  std::unordered_map<int64_t, uint32_t> at;
+  for (uint32_t i = 0; i < f.vtx.size(); ++i) at[key(f.vtx[i], R)] = i;
+  auto child = [&](const std::vector<uint32_t>& parent, int pdim, const Pt* pts, int n) {
+    std::vector<uint32_t> c(n);
+    for (int i = 0; i < n; ++i) c[i] = at.at(key(point(m, parent, pdim, pts[i]), R));
+    return c;
+  };
+  // edges: of edges, of quads, of hexas
+  for (auto& e : m.ent[1]) {
+    const uint32_t x = at.at(key(point(m, e, 1, {'x', 0}), R));
+    f.ent[1].push_back({e[0], x});
+    f.ent[1].push_back({x, e[1]});
+  }
+  for (auto& q : m.ent[2])
+    for (auto& r : kQuadEdges) f.ent[1].push_back(child(q, 2, r, 2));
+  if (m.dim == 3)
+    for (auto& h : m.ent[3])
+      for (auto& r : kHexaEdges) f.ent[1].push_back(child(h, 3, r, 2));
+  // quads: of quads, of hexas
+  for (auto& q : m.ent[2])
+    for (auto& r : kQuadQuads) f.ent[2].push_back(child(q, 2, r, 4));
+  if (m.dim == 3) {
+    for (auto& h : m.ent[3])
+      for (auto& r : kHexaQuads) f.ent[2].push_back(child(h, 3, r, 4));
+    for (auto& h : m.ent[3])
+      for (auto& r : kHexaHexas) f.ent[3].push_back(child(h, 3, r, 8));
+  }
+  return f;
+}
+}  // namespace numbering
+}  // namespace
+
+extern "C" int or_feat_numbering(int dim, int degree, int level, uint32_t* dof_lex, uint32_t* cell_lex) {
+  using namespace numbering;
+  if ((dim != 2 && dim != 3) || (degree != 1 && degree != 2) || level < 0 || level > (dim == 2 ? 12 : 8)) return -1;
+  const int64_t R = int64_t(1) << (level + 1);  // coordinates at twice the level's resolution
+  Mesh m = unit_cube(dim, R);
+  for (int l = 0; l < level; ++l) m = refine(m, R);
+  const int64_t N = int64_t(1) << level;
+  if (dof_lex) {
+    // DOF coordinates: vertices, then (Q2) the centres of edges, quads, hexas
+    std::vector<C3> dofs = m.vtx;
+    static const int all[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    if (degree == 2)
+      for (int d = 1; d <= dim; ++d)
+        for (auto& vs : m.ent[d]) dofs.push_back(centre(m, vs, all, 1 << d));
+    const int64_t M = degree * N + 1, scale = 2 / degree;  // lattice points per side, coordinate step
+    for (size_t f = 0; f < dofs.size(); ++f) {
+      int64_t idx = 0, stride = 1;
+      for (int a = 0; a < dim; ++a) { idx += dofs[f].c[a] / scale * stride; stride *= M; }
+      dof_lex[f] = uint32_t(idx);
+    }
+  }
+  if (cell_lex) {
+    const int64_t h = R / N;
+    for (size_t c = 0; c < m.ent[dim].size(); ++c) {
+      int64_t lo[3] = {R, R, R};
+      for (uint32_t v : m.ent[dim][c])
+        for (int a = 0; a < dim; ++a) lo[a] = std::min(lo[a], m.vtx[v].c[a]);
+      int64_t idx = 0, stride = 1;
+      for (int a = 0; a < dim; ++a) { idx += lo[a] / h * stride; stride *= N; }
+      cell_lex[c] = uint32_t(idx);
+    }
+  }
+  return 0;
+}

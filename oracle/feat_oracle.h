@@ -85,6 +85,13 @@ void or_csr_apply(double* r, double a, const double* x, double b, const double* 
                   const double* val, const int32_t* col, const int64_t* rowptr,
                   int64_t rows, int64_t cols, int transposed);
 
+/* FEAT3's numbering of the unit square / cube refined `level` times
+ * (RefinedUnitCubeFactory = UnitCubeFactory + StandardRefinery, common_factories.hpp:71-235,
+ * conformal_mesh.hpp:439-528): dof_lex[f] = lexicographic lattice index of FEAT DOF f of the
+ * Q1 (degree 1) or Q2 (degree 2) space, cell_lex[c] = lexicographic index of FEAT cell c.
+ * Either pointer may be NULL. Returns 0, or -1 for unsupported arguments. */
+int or_feat_numbering(int dim, int degree, int level, uint32_t* dof_lex, uint32_t* cell_lex);
+
 #ifdef __cplusplus
 }
 #endif

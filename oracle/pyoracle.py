@@ -60,6 +60,8 @@ def lib():
         L.or_vcycle.argtypes = [vp, vp, vp, vp]
         L.or_element_grad.argtypes = [vp, vp, vp, vp]
         L.or_csr_apply.argtypes = [vp, d, vp, d, vp, vp, vp, vp, i64, i64, i32]
+        L.or_feat_numbering.restype = i32
+        L.or_feat_numbering.argtypes = [i32, i32, i32, vp, vp]
         _lib = L
     return _lib
 
@@ -178,6 +180,17 @@ def csr_apply(a, x, b, y, rp, ci, va, rows, cols, transposed=False):
 
 # ---------------------------------------------------------------------------------------
 # the reference's own solver (oracle/_ref/feat_ref), when built
+def feat_numbering(dim, degree, level):
+    """(dof_lex, cell_lex): lexicographic index of each FEAT DOF / cell of the unit square or
+    cube refined `level` times (or_feat_numbering)"""
+    n = degree * (1 << level) + 1
+    dofs = np.zeros(n ** dim, dtype=np.uint32)
+    cells = np.zeros((1 << level) ** dim, dtype=np.uint32)
+    if lib().or_feat_numbering(dim, degree, level, _p(dofs), _p(cells)) != 0:
+        raise ValueError("unsupported numbering arguments")
+    return dofs, cells
+
+
 def have_ref():
     return os.path.exists(REF_BIN)
 

@@ -589,6 +589,11 @@ namespace RefDriver
           const Index N = Index(1) << lv.lvl;
           const auto lat = dof_lattice(lv, N);
           write_u64(pre + ".lattice", std::vector<unsigned long>(lat.begin(), lat.end()));
+          // lexicographic index of each of the level's cells, in FEAT's cell numbering
+          std::vector<unsigned long> cells(lv.mesh.get_num_elements());
+          for(Index c(0); c < lv.mesh.get_num_elements(); ++c)
+            cells[c] = cell_lex(lv.mesh, c, N);
+          write_u64(pre + ".cells", cells);
           if(i + 1 < levels.size())
           {
             dump_csr(pre + ".P", lv.transfer.get_mat_prol());

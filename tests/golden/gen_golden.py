@@ -8,6 +8,7 @@ lattice numbering through the DOF coordinates, as compressed .npz files:
     python tests/golden/gen_golden.py          # needs oracle/_ref/feat_ref
     python tests/golden/gen_golden.py --cycles # only the F/W-cycle and adaptive-CGC fixtures
     python tests/golden/gen_golden.py --files  # only the container-file fixtures (feat_files_q1_2d_L3/)
+    python tests/golden/gen_golden.py --numbering  # only FEAT's DOF and cell numbering (ref_numbering.npz)
 
 Inputs that are random (coefficient fields, target noise) are drawn here with numpy's
 seeded generator and stored in the fixture next to the outputs.
@@ -89,6 +90,21 @@ def feat_files():
     print(f"{out}: {len(names)} files, {total / 1024:.1f} KiB")
 
 
+def numbering():
+    """FEAT's own DOF and cell numbering of the refined unit square / cube, per level, as the
+    lexicographic lattice index of each FEAT DOF (from its interpolated coordinates) and of each
+    FEAT cell (from its centroid)"""
+    arrays = {}
+    for dim, degree, lmax in ((2, 1, 5), (2, 2, 4), (3, 1, 4), (3, 2, 3)):
+        R = po.run_ref(dim, degree, lmax, 1, rhs="sine", solver="pcg", nu=2, coarse="direct", tol=1e-6,
+                       dump_matrices=True)
+        pre = R["prefix"]
+        for l in range(1, lmax + 1):
+            arrays[f"d{dim}_q{degree}_L{l}_dofs"] = np.fromfile(f"{pre}.L{l}.lattice", dtype=np.uint64).astype(np.uint32)
+            arrays[f"d{dim}_q{degree}_L{l}_cells"] = np.fromfile(f"{pre}.L{l}.cells", dtype=np.uint64).astype(np.uint32)
+    save("ref_numbering", **arrays)
+
+
 def main():
     if not po.have_ref():
         sys.exit("oracle/_ref/feat_ref is missing: build it with `make -C oracle ref` first")
@@ -96,6 +112,8 @@ def main():
         return cycles()
     if "--files" in sys.argv:
         return feat_files()
+    if "--numbering" in sys.argv:
+        return numbering()
     rng = np.random.default_rng(20261203)
     # applications/poisson_dirichlet.cpp composition, level 5, the reference's pin (4 +- 1 iterations,
     # applications/CMakeLists.txt:100-108)
@@ -144,6 +162,7 @@ def main():
     save("ref_matrices_q1_2d_L3", **arrays)
     cycles()
     feat_files()
+    numbering()
 
 
 if __name__ == "__main__":

@@ -35,7 +35,7 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert lib.fb_csr_apply_f64(None, 1.0, None, 1.0, None, None, None, None, 5, 5, 5, 0, None) == _lib.FB_ERR_INVALID
     assert lib.fb_mg_create_structured(None, None) == _lib.FB_ERR_INVALID
     h = ctypes.c_void_p()
-    bad = _lib.StructuredDesc(4, 1, 3, 1, None, 0, 1)
+    bad = _lib.StructuredDesc(4, 1, 3, 1, None, 0, 1, 0)
     assert lib.fb_mg_create_structured(ctypes.byref(h), ctypes.byref(bad)) == _lib.FB_ERR_INVALID
     cfg = _lib.SolverCfg()
     lib.fb_solver_cfg_default(ctypes.byref(cfg))
