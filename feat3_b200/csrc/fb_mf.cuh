@@ -14,6 +14,10 @@
 // formed by the same warps with direct loads before they take their first tile, while the
 // producer's first copies are in flight.
 //
+// The direct-path rows all lie on the lattice boundary. When the level's filter is exactly that
+// boundary (structured hierarchies), every epilogue discards the product of a filtered row
+// (Jacobi keeps x, the defect and PCG's q are zero), so the kernel skips their 27-point gathers.
+//
 // Every wait on an mbarrier is bounded (about one second of %globaltimer); on expiry the
 // kernel records the event in `kerr`, stops taking tiles, waits (bounded) for its copies in
 // flight and returns, so the host can report the failure with the context intact.
@@ -101,6 +105,8 @@ struct MfTile {
   uint32_t nbl_items;    // direct-path items: boundary-line chunks
   uint32_t nedge_items;  // direct-path items: 16 interior lines' end points each
   uint32_t dz, dyt;      // grid stride in tiles, as (planes, tiles within a plane) = divmod(gridDim, tpp)
+  uint32_t direct_masked;  // the filter is the lattice boundary: every direct-path row is filtered, and
+                           // the epilogue of a filtered row does not read the product
 };
 
 // tiles of a block in grid-stride order without divisions in the loop
@@ -338,7 +344,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
           }
         }
         if (row >= 0) {
-          const T s = mf_row_direct<T>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
+          const T s = G.direct_masked ? T(0) : mf_row_direct<T>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
           acc += epi(uint32_t(row), s);
         }
       }

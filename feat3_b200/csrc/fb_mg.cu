@@ -475,6 +475,7 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   G.stage_bytes = (3 * G.cap_x + 2 * G.cap_k + NS * G.cap_s + G.cap_m + 127) & ~127u;
   G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
   G.nedge_items = (W * W + 15) / 16;
+  G.direct_masked = (L.mask_boundary && L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
   const size_t dyn = size_t(NST) * G.stage_bytes;
   auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
