@@ -588,9 +588,14 @@ __global__ void __launch_bounds__(256) k_rest_q1(Q1Transfer g, const T* __restri
 // loads (indices clamped; a clamped value always meets weight 0), then every thread forms CZ
 // coarse rows from shared memory. Terms and their order are those of k_rest_q1.
 // Launched on a (ceil(Mc1/32), ceil(Mc1/8), ceil(Mc1/CZ)) grid of 256 threads.
+//
+// bmask (structured levels, the filter is the lattice boundary): the grid covers the coarse
+// indices 0..Mc1-2 per axis only, so no block exists for the last plane, line or column alone
+// (2^l + 1 points per side). Those rows are filtered, hence zero; the threads next to them write
+// them without any fine data.
 template<typename T, int CZ>
 __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __restrict__ xf, EpiRestrict<T> epi,
-                                                      double* ws, unsigned* counter, double* red_out) {
+                                                      double* ws, unsigned* counter, double* red_out, int bmask) {
   constexpr int SX = 65, SY = 17, SZ = 2 * CZ + 1;
   pdl_wait();
   __shared__ T sm[SZ][SY][SX];
@@ -655,6 +660,28 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
           for (int c = 0; c < 3; ++c) s += (wxy[b][c] * wz[a]) * sm[2 * cz + a][2 * ty + b][2 * tx + c];
       const uint32_t i = uint32_t(X) + g.Mc1 * (uint32_t(Y) + g.Mc1 * uint32_t(Z));
       acc += epi(i, s);
+    }
+    if (bmask) {
+      // the boundary rows beyond the grid: X = Mc1-1 / Y = Mc1-1 next to this thread, and the
+      // plane Z = Mc1-1 above the last block
+      const int E = int(g.Mc1) - 1;
+      const bool ex = X == E - 1 && E == 32 * int(gridDim.x);
+      const bool ey = Y == E - 1 && E == 8 * int(gridDim.y);
+      const bool ez = int(blockIdx.z) == int(gridDim.z) - 1 && E == CZ * int(gridDim.z);
+      if (ex || ey || ez) {
+        const int nz = ez ? CZ + 1 : CZ;
+        for (int cz = 0; cz < nz; ++cz) {
+          const int Z = cz < CZ ? Z0 + cz : E;
+          if (Z > E) break;
+          for (int q = 0; q < 4; ++q) {
+            const bool qx = q & 1, qy = q & 2;
+            if ((qx && !ex) || (qy && !ey)) continue;
+            if (!qx && !qy && Z != E) continue;  // the thread's own row: formed above
+            const uint32_t i = uint32_t(qx ? E : X) + g.Mc1 * (uint32_t(qy ? E : Y) + g.Mc1 * uint32_t(Z));
+            acc += epi(i, T(0));
+          }
+        }
+      }
     }
   }
   const double blk = block_sum<256>(acc, sh);
