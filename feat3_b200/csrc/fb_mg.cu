@@ -253,10 +253,13 @@ __global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __res
 // has found ||r|| finite and above the tolerance, and a skipped smoother with nu >= 2 is
 // restored by the second step, which sees the same skip test).
 template<bool LOW>
-__global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float* r32, const double* __restrict__ p,
-                                                    const double* __restrict__ q, DevScalars* sc, uint32_t n,
-                                                    double* ws, unsigned* counter, double* rr_out,
-                                                    void* s1, const void* invd, const uint32_t* mask, double omega) {
+// The x update x += alpha p of this step is deferred to the next k_pcg_dir, which reads p
+// anyway before overwriting it (or to k_pcg_finish after the last iteration): the same
+// operation on the same values, one pass over p fewer per iteration.
+__global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const double* __restrict__ q,
+                                                    DevScalars* sc, uint32_t n, double* ws, unsigned* counter,
+                                                    double* rr_out, void* s1, const void* invd, const uint32_t* mask,
+                                                    double omega) {
   using T = typename std::conditional<LOW, float, double>::type;
   pdl_wait();
   __shared__ double sh[8];
@@ -271,7 +274,6 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double ri = r[i];
     if (upd) {
-      x[i] = alpha * p[i] + x[i];
       ri = (-alpha) * q[i] + ri;
       r[i] = ri;
     }
@@ -281,7 +283,18 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* x, double* r, float*
   }
   pdl_trigger();
   const double blk = block_sum<256>(acc, sh);
-  if (reduce_finish<256>(blk, ws, counter, rr_out, sh, false)) sc->gamma = sc->rz;
+  if (reduce_finish<256>(blk, ws, counter, rr_out, sh, false)) {
+    sc->gamma = sc->rz;
+    sc->alpha = upd ? alpha : 0.0;
+  }
+}
+
+// the x update of the last PCG step (pcg.hpp:256)
+__global__ void k_pcg_finish(double* x, const double* __restrict__ p, const DevScalars* sc, uint32_t n) {
+  const double alpha = sc->alpha;
+  if (alpha == 0.0) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = alpha * p[i] + x[i];
 }
 
 // r . z with z in FP64 or FP32 (ConvertPrecond: z = double(z_inner))
@@ -298,17 +311,23 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
   reduce_finish<256>(blk, ws, counter, out, sh, false);
 }
 
-// p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update
+// p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update.
+// First the previous step's pending x += alpha p (pcg.hpp:256), on the old p.
 template<typename ZT>
-__global__ void k_pcg_dir(double* p, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+__global__ void k_pcg_dir(double* p, double* x, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
   pdl_wait();
   const double beta = sc->rz / sc->gamma;
   const bool upd = fabs(beta) >= eps_of<double>();
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    p[i] = upd ? beta * p[i] + double(z[i]) : double(z[i]);
+  const double alpha = sc->alpha;
+  const bool xup = alpha != 0.0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double pi = p[i];
+    if (xup) x[i] = alpha * pi + x[i];
+    p[i] = upd ? beta * pi + double(z[i]) : double(z[i]);
+  }
 }
 
-__global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; }
+__global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; sc->alpha = 0.0; }
 
 // adaptive coarse-grid correction factor (multigrid.hpp:1898-1925): MinEnergy
 // omega = (def . cor) / (tmp . cor), MinDefect omega = (def . tmp) / (tmp . tmp), tmp = A cor;
@@ -1109,9 +1128,9 @@ static int body(fb_mg* m) {
       m->launches++;
       FB_CHECK_LAUNCH();
     }
-    if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, (const float*)z,
+    if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const float*)z,
                                 (const DevScalars*)m->sc, n));
-    else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir<double>, dim3(ew_grid(n)), dim3(256), 0, m->p, (const double*)z,
+    else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir<double>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const double*)z,
                                 (const DevScalars*)m->sc, n));
     m->launches++;
     FB_CHECK_LAUNCH();
@@ -1120,11 +1139,11 @@ static int body(fb_mg* m) {
     Level& L0 = m->L[0];
     const bool fs = fuse_s1(m);
     if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_update<true>, dim3(occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1)),
-                                dim3(256), 0, m->xb, m->r, m->r32, (const double*)m->p, (const double*)m->q, m->sc, n,
+                                dim3(256), 0, m->r, m->r32, (const double*)m->q, m->sc, n,
                                 m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x32 : nullptr, (const void*)L0.invd32,
                                 (const uint32_t*)L0.mask, m->cfg.omega_rich));
     else     FB_CUDA(launch_pdl(m->stream, k_pcg_update<false>, dim3(occupancy_grid((const void*)k_pcg_update<false>, n / 32 + 1)),
-                                dim3(256), 0, m->xb, m->r, m->r32, (const double*)m->p, (const double*)m->q, m->sc, n,
+                                dim3(256), 0, m->r, m->r32, (const double*)m->q, m->sc, n,
                                 m->ws, m->counter, &m->sc->rr, fs ? (void*)L0.x64 : nullptr, (const void*)L0.invd64,
                                 (const uint32_t*)L0.mask, m->cfg.omega_rich));
     m->launches++;
@@ -1503,6 +1522,11 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
     d = std::sqrt(*m->host_rr);
     if (hist) hist[it] = d;
     status = st.analyse(it, d);
+  }
+  if (m->cfg.outer == FB_OUTER_PCG) {
+    k_pcg_finish<<<ew_grid(n), 256, 0, s>>>(m->xb, m->p, m->sc, n);
+    m->launches++;
+    FB_CHECK_LAUNCH();
   }
   if (perm) FB_TRY(perm_from_lattice(m, sol, m->xb, perm, n));
   else FB_CUDA(cudaMemcpyAsync(sol, m->xb, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));

@@ -13,6 +13,8 @@ struct DevScalars {
   double rz;            // latest r . z
   double gamma;         // previous r . z (PCG)
   double qp;            // q . p
+  double alpha;         // PCG step length whose x update is still pending (applied with the next
+                        // direction update, or after the last iteration); 0 = none
   double lvl[2 * kMaxLevels];  // [2l] ||rhs_l||^2, [2l+1] ||post-smoothing defect_l||^2
   double tmp[8];
 };
