@@ -554,6 +554,9 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
         dev = std::max(dev, std::fabs(m->kref_h[a * m->nloc + b] - m->kref_h[a ^ b]));
       }
     m->mf_ok = dev <= 1e-14 * mx;
+    if (m->dim == 3)
+      m->mf_faces0 = std::fabs(m->kref_h[1]) <= 1e-14 * mx && std::fabs(m->kref_h[2]) <= 1e-14 * mx &&
+                     std::fabs(m->kref_h[4]) <= 1e-14 * mx;
   }
   const int nl = d->level - d->level_min + 1;
   m->L.resize(nl);

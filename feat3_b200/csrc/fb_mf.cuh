@@ -423,7 +423,9 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
           }
           // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
           // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
-          // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b])
+          // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b]). The 6 face
+          // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
+          // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
           ksums(kw, 1, K[1]);
           T S[8];
 #pragma unroll
@@ -434,13 +436,15 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
             for (int dy = 0; dy < 3; ++dy)
 #pragma unroll
               for (int dx = 0; dx < 3; ++dx) {
-                const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
                 const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
+                if (r == 1 || r == 2 || r == 4) continue;
+                const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
                 S[r] += Kd * xw[dz][dy][dx];
               }
           T s = A.kr[0] * S[0];
 #pragma unroll
-          for (int r = 1; r < 8; ++r) s += A.kr[r] * S[r];
+          for (int r = 3; r < 8; ++r)
+            if (r != 4) s += A.kr[r] * S[r];
           const uint32_t row = r0 + (l0 + j) * M1 + X;
           T sv[NS > 0 ? NS : 1];
           if (NS > 0) sv[0] = ss[j * int(M1)];

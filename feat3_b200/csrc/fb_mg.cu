@@ -541,7 +541,8 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   }
   for (int j = 0; j < (DIM == 3 ? 27 : 9); ++j) v.off[j] = L.St.off[j];
   if constexpr (DIM == 3 && Staged<Epi>::kOk) {
-    if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err && !(m->cfg.flags & FB_FLAG_NO_TILED))
+    if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err && m->mf_faces0 &&
+        !(m->cfg.flags & FB_FLAG_NO_TILED))
       return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
   }
   auto fn = k_mf_q1<T, Epi, DIM>;

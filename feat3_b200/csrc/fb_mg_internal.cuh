@@ -106,6 +106,8 @@ struct fb_mg {
   int nloc = 0;
   double* kref = nullptr;        // unit-coefficient element matrix on [-1,1]^d (device)
   bool mf_ok = false;            // K_ref[a][b] == K_ref[0][a^b] (Q1 cube symmetry): matrix-free apply possible
+  bool mf_faces0 = false;        // 3D: K_ref[0][1], [0][2], [0][4] (edge-adjacent vertices) are of rounding
+                                 // size, as for the Laplacian: the tiled kernel leaves those terms out
   std::vector<double> kref_h;
   // coarse level as CSR (for the single-CTA CG coarse solver) and its work vectors
   fb::DevCsr coarse_csr;
