@@ -470,13 +470,11 @@ static int check_self_checks(fb_mg* m) {
 }
 
 // line-tiled staged launch (3D levels with at least 16 interior points per line)
-template<typename T, typename Epi, int TY>
+template<typename T, typename Epi, int TY, int NST, int MINB>
 static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
                               double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
-  constexpr int NST = 2;
-  constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
   const uint32_t M1 = L.M1, N = M1 - 1, W = M1 - 2;
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
   // a structured level's filter is its lattice boundary, which no tile row touches
@@ -519,12 +517,14 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   return FB_OK;
 }
 
-// lines per thread: 4 (FP32) / 3 (FP64); 2 lines on the smaller FP32 levels (more tiles per CTA)
-// measured no faster
+// lines per thread and CTAs per SM (measured on the 257^3 solve): FP32 6 lines, 2 CTAs (96
+// registers, no spills; 4 lines at 3 CTAs spilled and ran 2.5 % slower); FP64 2 lines, 2 CTAs
+// (4 % faster than 3 lines)
 template<typename T, typename Epi>
 static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
                            double* red_out) {
-  return launch_mf_tiled_ty<T, Epi, sizeof(T) == 4 ? 4 : 3>(m, L, v, x, epi, red_out);
+  if constexpr (sizeof(T) == 4) return launch_mf_tiled_ty<T, Epi, 6, 2, 2>(m, L, v, x, epi, red_out);
+  else return launch_mf_tiled_ty<T, Epi, 2, 2, 2>(m, L, v, x, epi, red_out);
 }
 
 template<typename T, typename Epi, int DIM>
