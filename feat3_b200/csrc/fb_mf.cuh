@@ -230,7 +230,9 @@ __device__ __forceinline__ void ksums(const T (&kw)[2][2][2], int c, T (&K)[3][3
 
 // ------------------------------------------------------------------ the tiled kernel
 // 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
-template<typename T, typename Epi, int NST, int MINB, int TY>
+// CM1: the lattice size as a compile-time constant (0: G.M1 at run time), which turns the
+// shared-memory offsets of the window walk into immediates on the levels that dominate.
+template<typename T, typename Epi, int NST, int MINB, int TY, int CM1>
 __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTile G, const T* __restrict__ x, Epi epi,
                                                            const T* st0, const T* st1, const uint32_t* mask,
                                                            double* ws, unsigned* counter, double* red_out,
@@ -251,7 +253,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  const uint32_t M1 = G.M1, N = G.N;
+  const uint32_t M1 = CM1 ? uint32_t(CM1) : G.M1, N = M1 - 1;
   const uint32_t W = M1 - 2;  // interior points per line
   // stage layout: x planes | k cell planes | streams | mask words
   const uint32_t off_k = 3 * G.cap_x, off_s = off_k + 2 * G.cap_k, off_m = off_s + NS * G.cap_s;

@@ -470,7 +470,7 @@ static int check_self_checks(fb_mg* m) {
 }
 
 // line-tiled staged launch (3D levels with at least 16 interior points per line)
-template<typename T, typename Epi, int TY, int NST, int MINB>
+template<typename T, typename Epi, int TY, int NST, int MINB, int CM1>
 static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
                               double* red_out) {
   using SE = Staged<Epi>;
@@ -494,7 +494,7 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   G.nedge_items = (W * W + 15) / 16;
   G.direct_masked = (L.mask_boundary && L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
   const size_t dyn = size_t(NST) * G.stage_bytes;
-  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY>;
+  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY, CM1>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
   if (dyn > attr) {
     FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
@@ -519,12 +519,15 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 
 // lines per thread and CTAs per SM (measured on the 257^3 solve): FP32 6 lines, 2 CTAs (96
 // registers, no spills; 4 lines at 3 CTAs spilled and ran 2.5 % slower); FP64 2 lines, 2 CTAs
-// (4 % faster than 3 lines)
+// (4 % faster than 3 lines). Levels 8 and 7 of the 3D hierarchy get the lattice size as a
+// compile-time constant (3.5 % faster solve than the run-time size).
 template<typename T, typename Epi>
 static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
                            double* red_out) {
-  if constexpr (sizeof(T) == 4) return launch_mf_tiled_ty<T, Epi, 6, 2, 2>(m, L, v, x, epi, red_out);
-  else return launch_mf_tiled_ty<T, Epi, 2, 2, 2>(m, L, v, x, epi, red_out);
+  constexpr int TY = sizeof(T) == 4 ? 6 : 2;
+  if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 257>(m, L, v, x, epi, red_out);
+  if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129>(m, L, v, x, epi, red_out);
+  return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 0>(m, L, v, x, epi, red_out);
 }
 
 template<typename T, typename Epi, int DIM>
