@@ -11,6 +11,18 @@
 
 namespace fb {
 
+// one element global -> shared without a register round trip (cp.async, sm_80+): a warp's
+// whole staging pass is in flight at once; complete with cp_async_wait_all() + a barrier
+template<typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "cp.async element of 4 or 8 bytes");
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  if constexpr (sizeof(T) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+
 // ------------------------------------------------------------------ value loads
 template<typename VT> struct ValLoad;
 template<> struct ValLoad<double> { __device__ __forceinline__ static double ld(const double* p) { return __ldg(p); } };
@@ -603,9 +615,8 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
   const int X0 = int(blockIdx.x) * 32, Y0 = int(blockIdx.y) * 8, Z0 = int(blockIdx.z) * CZ;
   const int F = int(g.Mf1) - 1;
   const int fx0 = 2 * X0 - 1, fy0 = 2 * Y0 - 1, fz0 = 2 * Z0 - 1;
-  // one warp per fine line segment of 65 values (no index division)
+  // one warp per fine line segment of 65 values (no index division), all copies in flight
   const int lane = threadIdx.x & 31, wrp = threadIdx.x >> 5;
-#pragma unroll 4
   for (int r = wrp; r < SY * SZ; r += 8) {
     const int ly = r % SY, lz = r / SY;
     int fy = fy0 + ly, fz = fz0 + lz;
@@ -618,10 +629,11 @@ __global__ void __launch_bounds__(256) k_rest_q1_tile(Q1Transfer g, const T* __r
       if (lx < SX) {
         int fx = fx0 + lx;
         fx = fx < 0 ? 0 : (fx > F ? F : fx);
-        sm[lz][ly][lx] = line[fx];
+        cp_async_elem(&sm[lz][ly][lx], line + fx);
       }
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int X = X0 + tx, Y = Y0 + ty;
@@ -722,10 +734,11 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
       const int ly = r % CY, lz = r / CY;
       if (lane < CX) {
         const uint32_t cx = min(cx0 + lane, Cm), cy = min(cy0 + ly, Cm), cz = min(cz0 + lz, Cm);
-        cm[lz][ly][lane] = xc[(size_t(cz) * g.Mc1 + cy) * g.Mc1 + cx];
+        cp_async_elem(&cm[lz][ly][lane], xc + (size_t(cz) * g.Mc1 + cy) * g.Mc1 + cx);
       }
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   pdl_trigger();
   if (!act) return;
