@@ -522,14 +522,17 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 // (4 % faster than 3 lines), except PCG's q = A p with no streamed inputs: 3 lines (123 us per
 // level-8 launch against 149 us with 2 lines and 222 us with 1). Levels 8 and 7 of the 3D
 // hierarchy get the lattice size as a compile-time constant (3.5 % faster solve than the
-// run-time size).
+// run-time size). FP32 on the smaller levels (65^3 and below): 2 lines per thread (17.33 vs
+// 17.51 ms with 6; at 33^3 a plane of 31 lines is otherwise a single tile).
 template<typename T, typename Epi>
 static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
                            double* red_out) {
   constexpr int TY = sizeof(T) == 4 ? 6 : (std::is_same<Epi, EpiPcgQ<double>>::value ? 3 : 2);
   if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 257>(m, L, v, x, epi, red_out);
   if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129>(m, L, v, x, epi, red_out);
-  return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 0>(m, L, v, x, epi, red_out);
+  // the smaller levels have few lines per plane: short tiles spread them over more CTAs
+  constexpr int TYS = sizeof(T) == 4 ? 2 : TY;
+  return launch_mf_tiled_ty<T, Epi, TYS, 2, 2, 0>(m, L, v, x, epi, red_out);
 }
 
 template<typename T, typename Epi, int DIM>
