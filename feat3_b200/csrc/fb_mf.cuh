@@ -76,9 +76,9 @@ struct Staged<EpiDefect<T, RED, LOW>> {
   }
 };
 
-template<typename T>
-struct Staged<EpiPcgQ<T>> {
-  using E = EpiPcgQ<T>;
+template<typename T, typename PT>
+struct Staged<EpiPcgQ<T, PT>> {
+  using E = EpiPcgQ<T, PT>;
   static constexpr bool kOk = true;
   static constexpr int kStreams = 0;
   static const void* stream(const E&, int) { return nullptr; }
@@ -183,8 +183,8 @@ __device__ __forceinline__ void widen(uint64_t lo, uint64_t hi, uint64_t& alo, u
 
 // ------------------------------------------------------------------ direct-path row
 // A(k) x for one row at lattice point (X, Y, Z) with clamped gathers (any row of the level)
-template<typename T>
-__device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __restrict__ x, int32_t row, int32_t X,
+template<typename T, typename XT = T>
+__device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const XT* __restrict__ x, int32_t row, int32_t X,
                                            int32_t Y, int32_t Z) {
   const int32_t last = int32_t(A.rows) - 1;
   const int32_t N = int32_t(A.M1) - 1;
@@ -193,7 +193,7 @@ __device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const T* __res
   for (int j = 0; j < 27; ++j) {
     int32_t col = row + A.off[j];
     col = col < 0 ? 0 : (col > last ? last : col);
-    xv[j] = __ldg(x + col);
+    xv[j] = T(__ldg(x + col));
   }
   T s = T(0);
 #pragma unroll
@@ -232,14 +232,17 @@ __device__ __forceinline__ void ksums(const T (&kw)[2][2][2], int c, T (&K)[3][3
 // 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
 // CM1: the lattice size as a compile-time constant (0: G.M1 at run time), which turns the
 // shared-memory offsets of the window walk into immediates on the levels that dominate.
-template<typename T, typename Epi, int NST, int MINB, int TY, int CM1>
-__global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTile G, const T* __restrict__ x, Epi epi,
+// XT: storage type of the input vector x (FP32 for an FP64 product of an FP32-stored vector);
+// the window and the arithmetic are in T.
+template<typename T, typename Epi, int NST, int MINB, int TY, int CM1, typename XT = T>
+__global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTile G, const XT* __restrict__ x, Epi epi,
                                                            const T* st0, const T* st1, const uint32_t* mask,
                                                            double* ws, unsigned* counter, double* red_out,
                                                            unsigned* kerr) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr uint64_t E = 16 / sizeof(T);
+  constexpr uint64_t EX = 16 / sizeof(XT);
   pdl_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[NST], empty[NST];
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
       const void* src = nullptr;
       if (lane < 3) {
         const uint64_t zp = g.Z - 1 + lane;
-        widen<T>((zp * M1 + g.Y0 - 1) * M1, (zp * M1 + g.Y0 + g.lt) * M1 + M1 - 1, lo, by);
+        widen<XT>((zp * M1 + g.Y0 - 1) * M1, (zp * M1 + g.Y0 + g.lt) * M1 + M1 - 1, lo, by);
         src = x + lo;
         dst = lane * G.cap_x;
       } else if (lane < 5) {
@@ -346,7 +349,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
           }
         }
         if (row >= 0) {
-          const T s = G.direct_masked ? T(0) : mf_row_direct<T>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
+          const T s = G.direct_masked ? T(0) : mf_row_direct<T, XT>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
           acc += epi(uint32_t(row), s);
         }
       }
@@ -370,12 +373,12 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
       const uint32_t l0 = grp * TY;  // first line of this group, relative to Y0
       if (active && l0 < g.lt) {
         // window origin: x line Y0-1+l0 of each plane, k cell line Y0-1+l0, at this X
-        const T* xs[3];
+        const XT* xs[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
           const uint64_t zp = g.Z - 1 + q;
           const uint64_t xlo = (zp * M1 + g.Y0 - 1) * M1;
-          xs[q] = reinterpret_cast<const T*>(st + q * G.cap_x) + (xlo & (E - 1)) + l0 * M1 + X;
+          xs[q] = reinterpret_cast<const XT*>(st + q * G.cap_x) + (xlo & (EX - 1)) + l0 * M1 + X;
         }
         const T* ks[2] = {nullptr, nullptr};
         if (A.k) {
@@ -397,7 +400,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
 #pragma unroll
           for (int l = 0; l < 2; ++l)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) xw[q][l][d] = xs[q][l * int(M1) + d - 1];
+            for (int d = 0; d < 3; ++d) xw[q][l][d] = T(xs[q][l * int(M1) + d - 1]);
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           kw[q][0][0] = A.k ? ks[q][0] : T(1);
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
 #pragma unroll
           for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) xw[q][2][d] = xs[q][(j + 2) * int(M1) + d - 1];
+            for (int d = 0; d < 3; ++d) xw[q][2][d] = T(xs[q][(j + 2) * int(M1) + d - 1]);
           if (A.k) {
 #pragma unroll
             for (int q = 0; q < 2; ++q) {

@@ -290,11 +290,12 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const
 }
 
 // the x update of the last PCG step (pcg.hpp:256)
-__global__ void k_pcg_finish(double* x, const double* __restrict__ p, const DevScalars* sc, uint32_t n) {
+template<typename PT>
+__global__ void k_pcg_finish(double* x, const PT* __restrict__ p, const DevScalars* sc, uint32_t n) {
   const double alpha = sc->alpha;
   if (alpha == 0.0) return;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] = alpha * p[i] + x[i];
+    x[i] = alpha * double(p[i]) + x[i];
 }
 
 // r . z with z in FP64 or FP32 (ConvertPrecond: z = double(z_inner))
@@ -312,18 +313,21 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
 }
 
 // p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update.
-// First the previous step's pending x += alpha p (pcg.hpp:256), on the old p.
-template<typename ZT>
-__global__ void k_pcg_dir(double* p, double* x, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+// First the previous step's pending x += alpha p (pcg.hpp:256), on the old p. PT = float: the
+// direction is stored rounded to FP32 (the mixed matrix-free form); q = A p, x += alpha p and
+// q . p then all use the stored direction, so r stays the defect of x, and only the conjugacy
+// of successive directions carries the FP32 rounding, below that of the FP32 preconditioner.
+template<typename ZT, typename PT = double>
+__global__ void k_pcg_dir(PT* p, double* x, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
   pdl_wait();
   const double beta = sc->rz / sc->gamma;
   const bool upd = fabs(beta) >= eps_of<double>();
   const double alpha = sc->alpha;
   const bool xup = alpha != 0.0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double pi = p[i];
+    const double pi = double(p[i]);
     if (xup) x[i] = alpha * pi + x[i];
-    p[i] = upd ? beta * pi + double(z[i]) : double(z[i]);
+    p[i] = PT(upd ? beta * pi + double(z[i]) : double(z[i]));
   }
 }
 
@@ -470,8 +474,8 @@ static int check_self_checks(fb_mg* m) {
 }
 
 // line-tiled staged launch (3D levels with at least 16 interior points per line)
-template<typename T, typename Epi, int TY, int NST, int MINB, int CM1>
-static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
+template<typename T, typename Epi, int TY, int NST, int MINB, int CM1, typename XT = T>
+static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
                               double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
@@ -485,7 +489,7 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   G.Lt = G.G * TY;
   G.tpp = (W + G.Lt - 1) / G.Lt;
   G.ntiles = W * G.tpp;
-  G.cap_x = r16(uint64_t(G.Lt + 2) * M1 * sizeof(T)) + 32;
+  G.cap_x = r16(uint64_t(G.Lt + 2) * M1 * sizeof(XT)) + 32;
   G.cap_k = v.k ? r16(uint64_t(G.Lt + 1) * N * sizeof(T)) + 32 : 0;
   G.cap_s = NS ? r16(uint64_t(G.Lt) * M1 * sizeof(T)) + 32 : 0;
   G.cap_m = mask ? r16((uint64_t(G.Lt) * M1 / 32 + 2) * 4) + 32 : 0;
@@ -494,7 +498,7 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   G.nedge_items = (W * W + 15) / 16;
   G.direct_masked = (L.mask_boundary && L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
   const size_t dyn = size_t(NST) * G.stage_bytes;
-  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY, CM1>;
+  auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY, CM1, XT>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
   if (dyn > attr) {
     FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
@@ -524,15 +528,16 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 // hierarchy get the lattice size as a compile-time constant (3.5 % faster solve than the
 // run-time size). FP32 on the smaller levels (65^3 and below): 2 lines per thread (17.33 vs
 // 17.51 ms with 6; at 33^3 a plane of 31 lines is otherwise a single tile).
-template<typename T, typename Epi>
-static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const T* x, const Epi& epi,
+template<typename T, typename Epi, typename XT = T>
+static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
                            double* red_out) {
-  constexpr int TY = sizeof(T) == 4 ? 6 : (std::is_same<Epi, EpiPcgQ<double>>::value ? 3 : 2);
-  if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 257>(m, L, v, x, epi, red_out);
-  if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129>(m, L, v, x, epi, red_out);
+  constexpr bool pcgq = std::is_same<Epi, EpiPcgQ<double>>::value || std::is_same<Epi, EpiPcgQ<double, float>>::value;
+  constexpr int TY = sizeof(T) == 4 ? 6 : (pcgq ? 3 : 2);
+  if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 257, XT>(m, L, v, x, epi, red_out);
+  if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129, XT>(m, L, v, x, epi, red_out);
   // the smaller levels have few lines per plane: short tiles spread them over more CTAs
   constexpr int TYS = sizeof(T) == 4 ? 2 : TY;
-  return launch_mf_tiled_ty<T, Epi, TYS, 2, 2, 0>(m, L, v, x, epi, red_out);
+  return launch_mf_tiled_ty<T, Epi, TYS, 2, 2, 0, XT>(m, L, v, x, epi, red_out);
 }
 
 template<typename T, typename Epi, int DIM>
@@ -563,6 +568,28 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   FB_CHECK_LAUNCH();
   if (v.err && debug_enabled()) FB_TRY(check_self_checks(m));
   return FB_OK;
+}
+
+// The mixed matrix-free form keeps PCG's search direction in FP32 (half the bytes of p in the
+// direction update and in q = A p; the product itself in FP64): 3D levels the tiled kernel takes.
+static bool pcg_p32(const fb_mg* m) {
+  if (m->cfg.outer != FB_OUTER_PCG || m->cfg.precision == FB_PREC_F64 || m->dim != 3) return false;
+  const Level& L = m->L[0];
+  return use_matfree(m, L) && L.M1 >= 18 && L.n < (1u << 31) && m->mf_faces0 && !check_enabled() &&
+         !(m->cfg.flags & FB_FLAG_NO_TILED);
+}
+
+// q = filter_def(A p) and q . p with p stored in FP32, A(k) in FP64 (finest level)
+static int pcgq_p32(fb_mg* m, double* red) {
+  const Level& L = m->L[0];
+  MfView<double, 3> v;
+  v.rows = L.n; v.nchunks = (L.n + 31) / 32; v.M1 = L.M1; v.ne = L.ne;
+  v.err = nullptr;
+  v.k = L.k;
+  for (int r = 0; r < 8; ++r) v.kr[r] = L.kr64[r];
+  for (int j = 0; j < 27; ++j) v.off[j] = L.St.off[j];
+  EpiPcgQ<double, float> eq{m->q, m->p32, L.mask};
+  return launch_mf_tiled<double, EpiPcgQ<double, float>, float>(m, L, v, (const float*)m->p32, eq, red);
 }
 
 // level operator A x with an epilogue, on the storage the configuration selects
@@ -1137,14 +1164,21 @@ static int body(fb_mg* m) {
       m->launches++;
       FB_CHECK_LAUNCH();
     }
-    if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const float*)z,
-                                (const DevScalars*)m->sc, n));
+    const bool p32 = pcg_p32(m);
+    if (p32) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float, float>, dim3(ew_grid(n)), dim3(256), 0, m->p32, m->xb,
+                                (const float*)z, (const DevScalars*)m->sc, n));
+    else if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const float*)z,
+                                     (const DevScalars*)m->sc, n));
     else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir<double>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const double*)z,
                                 (const DevScalars*)m->sc, n));
     m->launches++;
     FB_CHECK_LAUNCH();
-    EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
-    FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
+    if (p32) {
+      FB_TRY(pcgq_p32(m, &m->sc->qp));
+    } else {
+      EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
+      FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
+    }
     Level& L0 = m->L[0];
     const bool fs = fuse_s1(m);
     if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_update<true>, dim3(occupancy_grid((const void*)k_pcg_update<true>, n / 32 + 1)),
@@ -1293,6 +1327,7 @@ static int ensure_vectors(fb_mg* m, int prec) {
   const uint32_t n = m->L[0].n;
   if (!m->r) {
     FB_TRY(dalloc(m, &m->r, n)); FB_TRY(dalloc(m, &m->p, n)); FB_TRY(dalloc(m, &m->q, n));
+    FB_TRY(dalloc(m, &m->p32, n));
     FB_TRY(dalloc(m, &m->xb, n)); FB_TRY(dalloc(m, &m->bb, n));
   }
   if (low && !m->r32) FB_TRY(dalloc(m, &m->r32, n));
@@ -1502,7 +1537,8 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
   FB_TRY(outer_defect(m));
   if (m->cfg.outer == FB_OUTER_PCG) {
     k_init_pcg<<<1, 1, 0, s>>>(m->sc);
-    k_fill<double><<<ew_grid(n), 256, 0, s>>>(m->p, 0.0, n);
+    if (pcg_p32(m)) k_fill<float><<<ew_grid(n), 256, 0, s>>>(m->p32, 0.0f, n);
+    else k_fill<double><<<ew_grid(n), 256, 0, s>>>(m->p, 0.0, n);
     m->launches += 2;
     FB_CHECK_LAUNCH();
     if (fuse_s1(m)) {
@@ -1533,7 +1569,8 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
     status = st.analyse(it, d);
   }
   if (m->cfg.outer == FB_OUTER_PCG) {
-    k_pcg_finish<<<ew_grid(n), 256, 0, s>>>(m->xb, m->p, m->sc, n);
+    if (pcg_p32(m)) k_pcg_finish<float><<<ew_grid(n), 256, 0, s>>>(m->xb, m->p32, m->sc, n);
+    else k_pcg_finish<double><<<ew_grid(n), 256, 0, s>>>(m->xb, m->p, m->sc, n);
     m->launches++;
     FB_CHECK_LAUNCH();
   }

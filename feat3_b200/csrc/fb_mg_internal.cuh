@@ -119,6 +119,7 @@ struct fb_mg {
   float* cinv32 = nullptr;
   // outer (finest) vectors
   double *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *xb = nullptr, *bb = nullptr;
+  float* p32 = nullptr;          // FP32 search direction of the mixed matrix-free form
   float* r32 = nullptr;
   // scalars / reduction workspace
   fb::DevScalars* sc = nullptr;

@@ -120,10 +120,12 @@ struct EpiJacobi {
 };
 
 // PCG direction product: q = filter_def(A p), reduction q . p
-template<typename T>
+// (p may be stored in FP32 when the outer solver keeps its search direction in FP32; the product
+// and q stay in T)
+template<typename T, typename PT = T>
 struct EpiPcgQ {
   static constexpr bool kReduce = true;
-  T* q; const T* p; const uint32_t* mask;
+  T* q; const PT* p; const uint32_t* mask;
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
     const T v = masked(mask, row) ? T(0) : s;
     q[row] = v;
