@@ -290,6 +290,7 @@ def native_arm(args):
     rf = {}
     for name, prec, fmt, which in (
             ("matfree_jacobi_f32", "f32", "matfree", 0), ("matfree_pcgq_f64", "f64", "matfree", 2),
+            ("matfree_pcgq_p32", "f32", "matfree", 3),
             ("stencil_jacobi_f16", "f16", "stencil", 0), ("stencil_jacobi_f64", "f64", "stencil", 0),
             ("stencil_pcgq_f64", "f64", "stencil", 2), ("sell_jacobi_f64", "f64", "sell", 0),
             ("sell_pcgq_f64", "f64", "sell", 2), ("sell_jacobi_f16", "f16", "sell", 0)):
@@ -298,8 +299,10 @@ def native_arm(args):
         _lib.call("fb_mg_time_spmv", mg.h, 0, which, {"f64": 0, "f32": 1, "f16": 2}[prec], 20, C.byref(ms))
         sx = 8 if prec == "f64" else 4                    # vector element size
         vec = n * sx * (3 if which == 0 else 1)           # Jacobi: rhs, invd, out; PCG q: q (p is the input)
+        if which == 3:                                    # FP32 direction in, FP64 q out, FP64 coefficients
+            vec = n * 8
         if fmt == "matfree":
-            mat = ne * sx                                 # per-cell coefficient instead of a matrix
+            mat = ne * (8 if which == 3 else sx)          # per-cell coefficient instead of a matrix
         else:
             sv = {"f64": 8, "f32": 4, "f16": 2}[prec]
             mat = nnz * (sv + (4 if fmt == "sell" else 0))  # values (+ 32-bit column indices)

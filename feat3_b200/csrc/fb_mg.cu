@@ -1762,7 +1762,7 @@ int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
 }
 
 int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* ms) {
-  if (!m || !ms || level < 0 || level >= (int)m->L.size() || reps < 1 || which < 0 || which > 2 || prec < 0 || prec > 2)
+  if (!m || !ms || level < 0 || level >= (int)m->L.size() || reps < 1 || which < 0 || which > 3 || prec < 0 || prec > 2)
     return FB_ERR_INVALID;
   if (!m->configured) return FB_ERR_NOT_READY;
   FB_CUDA(cudaSetDevice(m->device));
@@ -1776,6 +1776,10 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
   if (which == 2 && (level != 0 || low)) return FB_ERR_INVALID;
   const int saved = m->cfg.precision;
   m->cfg.precision = prec;
+  if (which == 3 && (level != 0 || !low || !pcg_p32(m))) {
+    m->cfg.precision = saved;
+    return FB_ERR_INVALID;
+  }
   FB_CUDA(cudaStreamSynchronize(m->stream));
   auto one = [&]() -> int {
     if (!low) {
@@ -1785,6 +1789,7 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
       EpiPcgQ<double> e{m->q, m->p, L.mask};
       return spmv_L<double>(m, L, (const double*)m->p, e, &m->sc->tmp[0]);
     }
+    if (which == 3) return pcgq_p32(m, &m->sc->tmp[0]);
     float* b = level == 0 ? m->r32 : L.rhs32;
     if (which == 0) { EpiJacobi<float, false> e{L.x32, b, L.invd32, L.y32, nullptr, L.mask, nullptr, float(m->cfg.omega_rich)}; return spmv_L<float>(m, L, L.x32, e, nullptr); }
     EpiDefect<float, false, false> e{L.def32, b, L.mask, nullptr};

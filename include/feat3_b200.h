@@ -300,7 +300,8 @@ FB_API int fb_mg_element_grad(fb_mg* mg, const double* u, const double* lambda, 
 /* Measurement helper: runs the level-`level` fused SpMV kernel `reps` times on the
  * hierarchy's stream between CUDA events and returns the mean device time per launch.
  * which: 0 = fused defect + Jacobi update (the smoother step), 1 = defect, 2 = PCG q = A p
- * with q.p; precision selects the value storage (FB_PREC_*). */
+ * with q.p, 3 = the same from the FP32-stored direction of the mixed matrix-free form (level 0,
+ * precision FB_PREC_F32); precision selects the value storage (FB_PREC_*). */
 FB_API int fb_mg_time_spmv(fb_mg* mg, int level, int which, int precision, int reps, double* ms_per_launch);
 
 /* ===================================================================================== */
