@@ -169,18 +169,54 @@ def reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------------------- ranks
+class Ranks:
+    """One process per GPU under torchrun (RANK / WORLD_SIZE / MASTER_* from the environment).
+    Replicas only: every rank solves its own copy of the problem; the process group carries the
+    barriers around the timed region and the max over ranks of each measured time, nothing of
+    the data path. backend/device: "nccl"/"cuda" for the bench, "gloo"/"cpu" in the tests."""
+
+    def __init__(self, backend="nccl", device="cuda", timeout_s=600):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+        if self.device == "cuda":
+            import torch
+            torch.cuda.synchronize()
+
+    def max(self, v):
+        """the job's time of a per-rank time: the slowest rank"""
+        if self.dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 # ------------------------------------------------------------------------------- native arm
 def native_arm(args):
     import torch
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ranks = Ranks("nccl", "cuda")
+    rank, world = ranks.rank, ranks.world
 
     from feat3_b200.solver import MultiGrid
     from feat3_b200 import _lib
@@ -195,17 +231,8 @@ def native_arm(args):
     rhs = mg.assemble_rhs("one")
     common = dict(outer="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     def run_form(prec, steps, warmup, host=False, fmt="stencil"):
         mg.configure(precision=prec, format=fmt, **common)
@@ -237,6 +264,7 @@ def native_arm(args):
         if rank == 0:
             print(json.dumps({"form": args.only, "time_s": float(np.median(t)), "iters": it[-1], "launches": l,
                               "dofs": n, "level": level}))
+        ranks.close()
         mg.close()
         return 0
     # --- FP64 forms: the drop-in (SELL-C-sigma, CSR transfers), the stencil storage, matrix-free
@@ -367,9 +395,7 @@ def native_arm(args):
             "wall_s_mixed_steps": wall,
         }
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     mg.close()
     return 0
 
