@@ -42,3 +42,21 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert (cfg.outer, cfg.nu, cfg.coarse, cfg.precision) == (0, 4, 0, 0)
     assert abs(cfg.tol_rel - 1e-8) < 1e-20 and abs(cfg.omega_jac - 0.5) < 1e-15
     assert lib.fb_mg_configure(None, ctypes.byref(cfg)) == _lib.FB_ERR_INVALID
+
+
+def test_plain_c_client_of_the_io_entry_points(tmp_path):
+    """the header compiles as C99 and a C program linked against the library round-trips the
+    reference's own files through fb_io_* (host code, no GPU)"""
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    exe = tmp_path / "io_client"
+    libdir = os.path.dirname(build.LIB)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I" + os.path.join(root, "include"),
+                    os.path.join(here, "capi_client", "io_client.c"), "-o", str(exe), "-L" + libdir, "-lfeat3_b200",
+                    "-Wl,-rpath," + libdir], check=True)
+    files = os.path.join(here, "golden", "feat_files_q1_2d_L3")
+    out = subprocess.run([str(exe), os.path.join(files, "L3.A.csr"), os.path.join(files, "rhs.dv"), str(tmp_path)],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    assert "matrix 81 x 81, 625 entries" in out.stdout and "vector 81 values" in out.stdout
