@@ -524,15 +524,18 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 // lines per thread and CTAs per SM (measured on the 257^3 solve): FP32 6 lines, 2 CTAs (96
 // registers, no spills; 4 lines at 3 CTAs spilled and ran 2.5 % slower); FP64 2 lines, 2 CTAs
 // (4 % faster than 3 lines), except PCG's q = A p with no streamed inputs: 3 lines (123 us per
-// level-8 launch against 149 us with 2 lines and 222 us with 1). Levels 8 and 7 of the 3D
-// hierarchy get the lattice size as a compile-time constant (3.5 % faster solve than the
-// run-time size). FP32 on the smaller levels (65^3 and below): 2 lines per thread (17.33 vs
-// 17.51 ms with 6; at 33^3 a plane of 31 lines is otherwise a single tile).
+// level-8 launch against 149 us with 2 lines and 222 us with 1); the same from the FP32-stored
+// direction, whose stages are smaller: 6 lines (101 us against 120 us with 3, 110 us with 4).
+// Levels 8 and 7 of the 3D hierarchy get the lattice size as a compile-time constant (3.5 %
+// faster solve than the run-time size). FP32 on the smaller levels (65^3 and below): 2 lines
+// per thread (17.33 vs 17.51 ms with 6; at 33^3 a plane of 31 lines is otherwise a single tile).
 template<typename T, typename Epi, typename XT = T>
 static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
                            double* red_out) {
-  constexpr bool pcgq = std::is_same<Epi, EpiPcgQ<double>>::value || std::is_same<Epi, EpiPcgQ<double, float>>::value;
-  constexpr int TY = sizeof(T) == 4 ? 6 : (pcgq ? 3 : 2);
+  // FP64 PCG-q from an FP64 direction: 3 lines; from the FP32 direction (smaller stages): 6
+  constexpr int TY = sizeof(T) == 4 ? 6
+                     : std::is_same<Epi, EpiPcgQ<double, float>>::value ? 6
+                     : std::is_same<Epi, EpiPcgQ<double>>::value ? 3 : 2;
   if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 257, XT>(m, L, v, x, epi, red_out);
   if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129, XT>(m, L, v, x, epi, red_out);
   // the smaller levels have few lines per plane: short tiles spread them over more CTAs
