@@ -115,6 +115,9 @@ _SIGS = {
     "fb_io_vector_serialised_size": [u64, C.POINTER(u64)],
     "fb_io_vector_serialise": [vp, u64, vp, u64],
     "fb_io_vector_deserialise": [vp, u64, C.POINTER(u64), C.POINTER(C.POINTER(dbl))],
+    "fb_io_sparse_vector_read": [C.c_char_p, i32, C.POINTER(u64), C.POINTER(u64), C.POINTER(C.POINTER(u64)),
+                                 C.POINTER(C.POINTER(dbl))],
+    "fb_io_sparse_vector_write": [C.c_char_p, i32, u64, u64, vp, vp],
     "fb_io_free": [vp],
     "fb_version": [],
 }

@@ -10,7 +10,9 @@
 //     (sparse_matrix_csr.hpp:1120-1241, 1296-1339), "array real general" for vectors
 //     (dense_vector.hpp:609-667, 744-759);
 //   * fm_exp             : one value per line, lines holding '#' skipped (dense_vector.hpp:
-//     669-705, 760-771).
+//     669-705, 760-771);
+//   * fm_mtx sparse vectors ("coordinate real general", one column): a UnitFilter's Dirichlet list
+//     (sparse_vector.hpp:517-680).
 // The byte layout has to be the reference's so that files cross between the two programs; the
 // parsing and formatting code is this library's own (a counting-sort CSR build instead of the
 // reference's ordered map, std::to_chars for the "%.6e" text of std::scientific).
@@ -480,6 +482,39 @@ int text_write_vector(FILE* f, const double* data, uint64_t n, bool mtx)
   return t.ok ? FB_OK : FB_ERR_IO;
 }
 
+// MatrixMarket sparse vectors ("coordinate real general", one column): the Dirichlet list of a
+// UnitFilter (SparseVector::read_from / write_out, kernel/lafem/sparse_vector.hpp:517-680).
+// Entries come back sorted by index; of repeated indices the last in the file is kept, as the
+// reference's sort() keeps it (sparse_vector.hpp:412-470).
+int mtx_read_sparse_vector(std::string& s, uint64_t& size, std::vector<uint64_t>& idx, std::vector<double>& val)
+{
+  Lines lines(s);
+  char* head = lines.next();
+  if(!head || !std::strstr(head, "%%MatrixMarket matrix coordinate real general")) return FB_ERR_FORMAT;
+  char* l = size_line(lines);
+  uint64_t rows, cols, nnz;
+  if(!l || !parse_index(l, rows) || !parse_index(l, cols) || !parse_index(l, nnz) || cols != 1) return FB_ERR_FORMAT;
+  std::vector<std::pair<uint64_t, double>> e;
+  while((l = lines.next()) != nullptr) {
+    if(blank(l)) continue;
+    uint64_t r, c;
+    if(!parse_index(l, r) || !parse_index(l, c) || r < 1 || r > rows) return FB_ERR_FORMAT;
+    e.emplace_back(r - 1, std::strtod(l, nullptr));
+  }
+  if(e.size() != nnz) return FB_ERR_FORMAT;
+  std::stable_sort(e.begin(), e.end(),
+                   [](const std::pair<uint64_t, double>& a, const std::pair<uint64_t, double>& b) { return a.first < b.first; });
+  idx.clear();
+  val.clear();
+  for(size_t i = 0; i < e.size(); ++i) {
+    if(i + 1 < e.size() && e[i + 1].first == e[i].first) continue;  // a later entry of the same index
+    idx.push_back(e[i].first);
+    val.push_back(e[i].second);
+  }
+  size = rows;
+  return FB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -616,6 +651,53 @@ FB_API int fb_io_vector_deserialise(const void* buf, uint64_t size, uint64_t* n,
   Parts p;
   const int rc = deserialise(static_cast<const char*>(buf), size, kMagicDv, p);
   return rc != FB_OK ? rc : dv_from_parts(p, n, data);
+}
+
+FB_API int fb_io_sparse_vector_read(const char* path, int mode, uint64_t* size, uint64_t* nnz, uint64_t** indices,
+                                    double** values)
+{
+  if(!size || !nnz || !indices || !values) return FB_ERR_INVALID;
+  *size = *nnz = 0;
+  *indices = nullptr;
+  *values = nullptr;
+  if(mode != FB_FILE_MTX) return FB_ERR_UNSUPPORTED;
+  std::string s;
+  int rc = read_file(path, s);
+  if(rc != FB_OK) return rc;
+  std::vector<uint64_t> idx;
+  std::vector<double> val;
+  if((rc = mtx_read_sparse_vector(s, *size, idx, val)) != FB_OK) return rc;
+  uint64_t* pi = alloc_copy<uint64_t>(idx.data(), idx.size());
+  double* pv = alloc_copy<double>(val.data(), val.size());
+  if(!pi || !pv) {
+    std::free(pi);
+    std::free(pv);
+    return FB_ERR_ALLOC;
+  }
+  *nnz = idx.size();
+  *indices = pi;
+  *values = pv;
+  return FB_OK;
+}
+
+FB_API int fb_io_sparse_vector_write(const char* path, int mode, uint64_t size, uint64_t nnz, const uint64_t* indices,
+                                     const double* values)
+{
+  if(mode != FB_FILE_MTX) return FB_ERR_UNSUPPORTED;
+  if(nnz && (!indices || !values)) return FB_ERR_INVALID;
+  for(uint64_t i = 0; i < nnz; ++i)
+    if(indices[i] >= size || (i > 0 && indices[i] <= indices[i - 1])) return FB_ERR_INVALID;
+  FILE* f;
+  int rc = open_write(path, true, f);
+  if(rc != FB_OK) return rc;
+  Text t(f);
+  t.str("%%MatrixMarket matrix coordinate real general\n");
+  t.u(size); t.str(" 1 "); t.u(nnz); t.ch('\n');
+  for(uint64_t i = 0; i < nnz; ++i) {
+    t.u(indices[i] + 1); t.str(" 1 "); t.d(values[i]); t.ch('\n');
+  }
+  t.flush();
+  return close_write(f, t.ok);
 }
 
 FB_API void fb_io_free(void* p)

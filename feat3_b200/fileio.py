@@ -10,6 +10,7 @@ FB_ERR_FORMAT for contents that do not match the mode), where the reference thro
     A = read_csr(FileMode.fm_csr, "level3.A.csr")       # SparseMatrixCSR::read_from
     write_csr(FileMode.fm_mtx, "level3.A.mtx", A)       # SparseMatrixCSR::write_out
     b = read_vector(FileMode.fm_dv, "rhs.dv")           # DenseVector::read_from
+    n, dirichlet, _ = read_sparse_vector(FileMode.fm_mtx, "level3.filter.mtx")  # UnitFilter's list
 """
 from __future__ import annotations
 
@@ -153,11 +154,39 @@ def deserialise_vector(data: bytes) -> np.ndarray:
     return _take_vector(n, out)
 
 
+def read_sparse_vector(mode, filename):
+    """SparseVector::read_from (sparse_vector.hpp:517-630), fm_mtx: (size, indices, values) with
+    0-based indices sorted ascending (a repeated index keeps its last value)"""
+    size, nnz = C.c_uint64(0), C.c_uint64(0)
+    idx, val = C.POINTER(C.c_uint64)(), C.POINTER(C.c_double)()
+    _lib.call("fb_io_sparse_vector_read", _path(filename), int(mode), C.byref(size), C.byref(nnz), C.byref(idx),
+              C.byref(val))
+    lib = _lib.load()
+    try:
+        n = nnz.value
+        i = np.ctypeslib.as_array(idx, shape=(n,)).copy() if n else np.zeros(0, np.uint64)
+        v = np.ctypeslib.as_array(val, shape=(n,)).copy() if n else np.zeros(0)
+    finally:
+        lib.fb_io_free(C.cast(idx, C.c_void_p))
+        lib.fb_io_free(C.cast(val, C.c_void_p))
+    return size.value, i.astype(np.uint64), v
+
+
+def write_sparse_vector(mode, filename, size, indices, values=None):
+    """SparseVector::write_out (sparse_vector.hpp:639-680), fm_mtx; values default to 0 (a
+    homogeneous Dirichlet list)"""
+    i = np.ascontiguousarray(indices, dtype=np.uint64)
+    v = np.zeros(i.size) if values is None else np.ascontiguousarray(values, dtype=np.float64)
+    _lib.call("fb_io_sparse_vector_write", _path(filename), int(mode), int(size), i.size,
+              i.ctypes.data if i.size else None, v.ctypes.data if v.size else None)
+
+
 def read_hierarchy(files):
     """Levels for ``MultiGrid.from_csr`` from FEAT3 matrix files, finest level first. ``files``
     holds one dict per level with the paths (or CsrFile objects) of 'A' and, except on the
-    coarsest level, 'P' and 'R', plus the Dirichlet DOF list 'filter'; a path ending in '.mtx'
-    is read as fm_mtx, any other as fm_binary."""
+    coarsest level, 'P' and 'R', plus the Dirichlet DOF list 'filter' (an index array, or the path
+    of the filter's sparse vector in fm_mtx); a matrix path ending in '.mtx' is read as fm_mtx,
+    any other as fm_binary."""
     def load(x):
         if isinstance(x, CsrFile):
             return x
@@ -166,7 +195,10 @@ def read_hierarchy(files):
 
     levels = []
     for f in files:
-        d = {"A": load(f["A"]).arrays(), "filter": np.asarray(f["filter"], dtype=np.uint64)}
+        flt = f["filter"]
+        if isinstance(flt, (str, bytes, os.PathLike)):
+            flt = read_sparse_vector(FileMode.fm_mtx, flt)[1]
+        d = {"A": load(f["A"]).arrays(), "filter": np.asarray(flt, dtype=np.uint64)}
         for key in ("P", "R"):
             if key in f:
                 d[key] = load(f[key]).arrays()

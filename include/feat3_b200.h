@@ -341,6 +341,16 @@ FB_API int fb_io_vector_write(const char* path, int mode, const double* data, ui
 FB_API int fb_io_vector_serialised_size(uint64_t n, uint64_t* size);
 FB_API int fb_io_vector_serialise(const double* data, uint64_t n, void* buf, uint64_t capacity);
 FB_API int fb_io_vector_deserialise(const void* buf, uint64_t size, uint64_t* n, double** data);
+/* Read / write a sparse vector as MatrixMarket "coordinate real general" with one column
+ * (FB_FILE_MTX only, as the reference), e.g. a UnitFilter's Dirichlet list
+ * (UnitFilter::get_filter_vector().write_out(fm_mtx, ...)). Read: indices 0-based, sorted, a
+ * repeated index keeps its last value; *indices and *values are freed with fb_io_free. Write:
+ * indices strictly ascending and < size. Replaces SparseVector::read_from / write_out
+ * (kernel/lafem/sparse_vector.hpp:517-680). */
+FB_API int fb_io_sparse_vector_read(const char* path, int mode, uint64_t* size, uint64_t* nnz, uint64_t** indices,
+                                    double** values);
+FB_API int fb_io_sparse_vector_write(const char* path, int mode, uint64_t size, uint64_t nnz, const uint64_t* indices,
+                                     const double* values);
 FB_API void fb_io_free(void* p);
 
 /* library version string */

@@ -429,6 +429,12 @@ namespace RefDriver
       MatrixType bin;
       bin.read_from(LAFEM::FileMode::fm_binary, pre + ".A.csr");
       bin.write_out(LAFEM::FileMode::fm_binary, pre + ".A.csr.csr");
+      // the Dirichlet filter's sparse vector (SparseVector::write_out / read_from,
+      // kernel/lafem/sparse_vector.hpp:517-680)
+      lv.filter.get_filter_vector().write_out(LAFEM::FileMode::fm_mtx, pre + ".filter.mtx");
+      LAFEM::SparseVector<Mem::Main, double, Index> fv;
+      fv.read_from(LAFEM::FileMode::fm_mtx, pre + ".filter.mtx");
+      fv.write_out(LAFEM::FileMode::fm_mtx, pre + ".filter.mtx.mtx");
       if(transfers)
       {
         lv.transfer.get_mat_prol().write_out(LAFEM::FileMode::fm_csr, pre + ".P.csr");

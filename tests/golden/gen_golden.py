@@ -71,8 +71,9 @@ def cycles():
 
 def feat_files():
     """The hierarchy of the 2D Q1 level-3 case (levels 3..1) as written by the reference's own
-    SparseMatrixCSR/DenseVector::write_out (sparse_matrix_csr.hpp:1261-1343, dense_vector.hpp:
-    721-777), and the reference's own parse of its text files written back in binary (*.mtx.csr,
+    SparseMatrixCSR/DenseVector/SparseVector::write_out (sparse_matrix_csr.hpp:1261-1343,
+    dense_vector.hpp:721-777, sparse_vector.hpp:639-680; the filters' Dirichlet lists), and the
+    reference's own parse of its text files written back in binary (*.mtx.csr,
     *.exp.dv, *.vmtx.dv; read_from, sparse_matrix_csr.hpp:1098-1246, dense_vector.hpp:587-712)."""
     R = po.run_ref(2, 1, 3, 1, rhs="sine", solver="pcg", nu=2, coarse="direct", tol=1e-8, feat_files=True)
     pre = R["prefix"]
@@ -80,6 +81,7 @@ def feat_files():
     os.makedirs(out, exist_ok=True)
     names = [f"L{l}.A.csr" for l in (1, 2, 3)] + [f"L{l}.{m}.csr" for l in (2, 3) for m in "PR"]
     names += ["L3.A.mtx", "L3.A.sym.mtx", "L3.A.mtx.csr", "L3.A.sym.mtx.csr", "L3.P.mtx", "L3.R.mtx"]
+    names += [f"L{l}.filter.mtx" for l in (1, 2, 3)]
     names += ["rhs.dv", "rhs.exp", "rhs.vmtx", "rhs.exp.dv", "rhs.vmtx.dv", "u.dv"]
     total = 0
     for nm in names:

@@ -14,8 +14,8 @@ import pytest
 
 from feat3_b200 import _lib
 from feat3_b200.fileio import (CsrFile, FileMode, deserialise_csr, deserialise_vector, read_csr,
-                               read_hierarchy, read_vector, serialise_csr, serialise_vector, write_csr,
-                               write_vector)
+                               read_hierarchy, read_sparse_vector, read_vector, serialise_csr, serialise_vector,
+                               write_csr, write_sparse_vector, write_vector)
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FILES = os.path.join(GOLD, "feat_files_q1_2d_L3")
@@ -112,6 +112,43 @@ def test_vectors_against_reference_files(dumps, tmp_path):
     # the reference's own parse of its text vectors
     assert serialise_vector(read_vector(FileMode.fm_exp, ff("rhs.exp"))) == raw("rhs.exp.dv")
     assert serialise_vector(read_vector(FileMode.fm_mtx, ff("rhs.vmtx"))) == raw("rhs.vmtx.dv")
+
+
+@pytest.mark.parametrize("level", [1, 2, 3])
+def test_filter_vectors_against_reference_files(level, dumps, tmp_path):
+    """the UnitFilter's Dirichlet list as the reference's SparseVector::write_out wrote it"""
+    size, idx, val = read_sparse_vector(FileMode.fm_mtx, ff(f"L{level}.filter.mtx"))
+    assert size == ((1 << level) + 1) ** 2
+    np.testing.assert_array_equal(idx, dumps[f"L{level}_filter"])
+    assert np.all(val == 0.0)
+    out = tmp_path / "f.mtx"
+    write_sparse_vector(FileMode.fm_mtx, out, size, idx, val)
+    assert out.read_bytes() == raw(f"L{level}.filter.mtx")
+
+
+def test_sparse_vector_reader_details(tmp_path):
+    """unsorted entries come back sorted; of a repeated index the last value is kept (the
+    reference's sort); the column must be 1 and the entry count must match the header"""
+    p = tmp_path / "s.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate real general\n% c\n10 1 4\n7 1 2.5\n2 1 -1\n7 1 3.5\n10 1 1e-3\n")
+    size, idx, val = read_sparse_vector(FileMode.fm_mtx, p)
+    assert size == 10
+    np.testing.assert_array_equal(idx, [1, 6, 9])
+    np.testing.assert_array_equal(val, [-1.0, 3.5, 1e-3])
+    for text in ("%%MatrixMarket matrix coordinate real general\n10 2 1\n1 1 1\n",      # two columns
+                 "%%MatrixMarket matrix coordinate real general\n10 1 2\n1 1 1\n",      # count
+                 "%%MatrixMarket matrix coordinate real general\n10 1 1\n11 1 1\n",     # range
+                 "%%MatrixMarket matrix array real general\n10 1\n1\n"):                # kind
+        p.write_text(text)
+        with pytest.raises(_lib.FeatError) as e:
+            read_sparse_vector(FileMode.fm_mtx, p)
+        assert status(e) == _lib.FB_ERR_FORMAT, text
+    with pytest.raises(_lib.FeatError) as e:
+        write_sparse_vector(FileMode.fm_mtx, tmp_path / "x.mtx", 5, [3, 1])
+    assert status(e) == _lib.FB_ERR_INVALID
+    with pytest.raises(_lib.FeatError) as e:
+        read_sparse_vector(FileMode.fm_csr, p)
+    assert status(e) == _lib.FB_ERR_UNSUPPORTED
 
 
 # ---------------------------------------------------------------------------------------------
@@ -281,12 +318,19 @@ def test_mode_and_argument_errors(tmp_path):
     assert status(e) == _lib.FB_ERR_IO
 
 
+FEAT_FILES = [{"A": "L3.A.csr", "P": "L3.P.csr", "R": "L3.R.csr", "filter": "L3.filter.mtx"},
+              {"A": "L2.A.csr", "P": "L2.P.csr", "R": "L2.R.csr", "filter": "L2.filter.mtx"},
+              {"A": "L1.A.csr", "filter": "L1.filter.mtx"}]
+
+
+def feat_files():
+    return [{k: ff(v) for k, v in lv.items()} for lv in FEAT_FILES]
+
+
 def test_hierarchy_from_files_matches_arrays(dumps):
-    files = [{"A": ff("L3.A.csr"), "P": ff("L3.P.csr"), "R": ff("L3.R.csr"), "filter": dumps["L3_filter"]},
-             {"A": ff("L2.A.csr"), "P": ff("L2.P.csr"), "R": ff("L2.R.csr"), "filter": dumps["L2_filter"]},
-             {"A": ff("L1.A.csr"), "filter": dumps["L1_filter"]}]
-    levels = read_hierarchy(files)
+    levels = read_hierarchy(feat_files())
     for lv, l in zip(levels, (3, 2, 1)):
+        np.testing.assert_array_equal(lv["filter"], dumps[f"L{l}_filter"])
         for mat in ("A", "P", "R"):
             if mat in lv:
                 for part, arr in zip(("rowptr", "col", "val"), lv[mat]):
@@ -296,13 +340,12 @@ def test_hierarchy_from_files_matches_arrays(dumps):
 @pytest.mark.gpu
 @pytest.mark.parametrize("sigma", [1, 256])
 def test_solve_on_hierarchy_read_from_reference_files(sigma, dumps):
-    """hierarchy exchange: the reference's files in, the reference's solution out"""
+    """hierarchy exchange: the reference's files in (matrices, transfers, Dirichlet lists, rhs),
+    the reference's solution out"""
     import torch
     from feat3_b200.solver import MultiGrid
-    files = [{"A": ff("L3.A.csr"), "P": ff("L3.P.csr"), "R": ff("L3.R.csr"), "filter": dumps["L3_filter"]},
-             {"A": ff("L2.A.csr"), "P": ff("L2.P.csr"), "R": ff("L2.R.csr"), "filter": dumps["L2_filter"]},
-             {"A": ff("L1.A.csr"), "filter": dumps["L1_filter"]}]
-    mg = MultiGrid.from_csr(read_hierarchy(files), sell_sigma=sigma).configure(nu=2, omega_jac=0.5, coarse="direct")
+    mg = MultiGrid.from_csr(read_hierarchy(feat_files()), sell_sigma=sigma).configure(nu=2, omega_jac=0.5,
+                                                                                     coarse="direct")
     rhs = read_vector(FileMode.fm_dv, ff("rhs.dv"))
     res = mg.solve(torch.tensor(rhs).cuda())
     u_ref = read_vector(FileMode.fm_dv, ff("u.dv"))
