@@ -4,7 +4,7 @@
  * Three layers:
  *  1. Operator layer: one entry point per FEAT3 backend function of the LAFEM arch
  *     boundary for Mem::CUDA (the headers of kernel/lafem/arch). A FEAT3 build binds
- *     LAFEM::Arch::<Op><Mem::CUDA> onto these, so the reference's
+ *     LAFEM::Arch::<Op><Mem::CUDA> onto these (one forwarding line each), so the reference's
  *     SparseMatrixCSR/SparseMatrixELL::apply, DenseVector::axpy/dot/norm2, UnitFilter and
  *     Transfer containers -- and the MultiGrid/PCG/Richardson templates above them -- run on
  *     these kernels unchanged.
