@@ -630,9 +630,17 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
         // coarse level l+1: its filter is the lattice boundary when structured
         const int bmask = m->L[l + 1].mask_boundary && epi.mask == m->L[l + 1].mask;
         const uint32_t E = L.tr.Mc1 - (bmask ? 1 : 0);  // indices the grid must cover
-        const dim3 grid((E + 31) / 32, (E + 7) / 8, (E + CZ - 1) / CZ);
-        FB_CUDA(launch_pdl(m->stream, k_rest_q1_tile<T, CZ>, grid, dim3(256), 0, L.tr, xf, epi, m->ws, m->counter, red,
-                           bmask));
+        // below 129^3 coarse points, 2 coarse planes per block spread the few blocks better
+        // (8.6 vs 12.2 us onto 17^3; 47.8 vs 50.4 us onto 129^3 stays with 4)
+        if (CZ == 4 && L.tr.Mc1 < 129) {
+          const dim3 g2((E + 31) / 32, (E + 7) / 8, (E + 1) / 2);
+          FB_CUDA(launch_pdl(m->stream, k_rest_q1_tile<T, 2>, g2, dim3(256), 0, L.tr, xf, epi, m->ws, m->counter, red,
+                             bmask));
+        } else {
+          const dim3 grid((E + 31) / 32, (E + 7) / 8, (E + CZ - 1) / CZ);
+          FB_CUDA(launch_pdl(m->stream, k_rest_q1_tile<T, CZ>, grid, dim3(256), 0, L.tr, xf, epi, m->ws, m->counter,
+                             red, bmask));
+        }
         m->launches++;
         FB_CHECK_LAUNCH();
         return FB_OK;
