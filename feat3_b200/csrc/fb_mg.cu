@@ -252,15 +252,21 @@ __global__ void __launch_bounds__(THREADS) k_coarse_cg(CsrView A, const T* __res
 // the smoother's skip test is not needed there: the next V-cycle runs only after the host
 // has found ||r|| finite and above the tolerance, and a skipped smoother with nu >= 2 is
 // restored by the second step, which sees the same skip test).
+template<typename T> struct Pair;
+template<> struct Pair<float> { using type = float2; };
+template<> struct Pair<double> { using type = double2; };
+
 template<bool LOW>
 // The x update x += alpha p of this step is deferred to the next k_pcg_dir, which reads p
 // anyway before overwriting it (or to k_pcg_finish after the last iteration): the same
-// operation on the same values, one pass over p fewer per iteration.
+// operation on the same values, one pass over p fewer per iteration. Two rows per thread and
+// step, with 8- and 16-byte accesses (all vectors are allocation bases, so pairs are aligned).
 __global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const double* __restrict__ q,
                                                     DevScalars* sc, uint32_t n, double* ws, unsigned* counter,
                                                     double* rr_out, void* s1, const void* invd, const uint32_t* mask,
                                                     double omega) {
   using T = typename std::conditional<LOW, float, double>::type;
+  using T2 = typename Pair<T>::type;
   pdl_wait();
   __shared__ double sh[8];
   // alpha = gamma' / (q . p) with gamma' = r . z of this iteration (pcg.hpp:241-251); the thread
@@ -271,7 +277,30 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const
   const T* invt = static_cast<const T*>(invd);
   const T om = T(omega);
   double acc = 0.0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t j = tid; j < n / 2; j += stride) {
+    const uint32_t i = 2 * j;
+    double2 rv = reinterpret_cast<const double2*>(r)[j];
+    if (upd) {
+      const double2 qv = __ldg(reinterpret_cast<const double2*>(q) + j);
+      rv.x = (-alpha) * qv.x + rv.x;
+      rv.y = (-alpha) * qv.y + rv.y;
+      reinterpret_cast<double2*>(r)[j] = rv;
+    }
+    if (LOW) reinterpret_cast<float2*>(r32)[j] = make_float2(float(rv.x), float(rv.y));
+    if (s1t) {
+      const uint32_t w = mask ? __ldg(mask + (i >> 5)) : 0u;  // i even: rows i, i+1 share the word
+      const T2 iv = reinterpret_cast<const T2*>(invt)[j];
+      T2 o;
+      o.x = ((w >> (i & 31)) & 1u) ? T(0) : om * (iv.x * T(rv.x));
+      o.y = ((w >> ((i + 1) & 31)) & 1u) ? T(0) : om * (iv.y * T(rv.y));
+      reinterpret_cast<T2*>(s1t)[j] = o;
+    }
+    acc += rv.x * rv.x;
+    acc += rv.y * rv.y;
+  }
+  if ((n & 1u) && tid == 0) {  // the last row of an odd count
+    const uint32_t i = n - 1;
     double ri = r[i];
     if (upd) {
       ri = (-alpha) * q[i] + ri;
@@ -319,12 +348,32 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
 // of successive directions carries the FP32 rounding, below that of the FP32 preconditioner.
 template<typename ZT, typename PT = double>
 __global__ void k_pcg_dir(PT* p, double* x, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+  using P2 = typename Pair<PT>::type;
+  using Z2 = typename Pair<ZT>::type;
   pdl_wait();
   const double beta = sc->rz / sc->gamma;
   const bool upd = fabs(beta) >= eps_of<double>();
   const double alpha = sc->alpha;
   const bool xup = alpha != 0.0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  // two rows per thread and step (allocation bases: pairs are aligned)
+  for (uint32_t j = tid; j < n / 2; j += stride) {
+    const P2 pv = reinterpret_cast<const P2*>(p)[j];
+    const Z2 zv = __ldg(reinterpret_cast<const Z2*>(z) + j);
+    const double p0 = double(pv.x), p1 = double(pv.y);
+    if (xup) {
+      double2 xv = reinterpret_cast<const double2*>(x)[j];
+      xv.x = alpha * p0 + xv.x;
+      xv.y = alpha * p1 + xv.y;
+      reinterpret_cast<double2*>(x)[j] = xv;
+    }
+    P2 o;
+    o.x = PT(upd ? beta * p0 + double(zv.x) : double(zv.x));
+    o.y = PT(upd ? beta * p1 + double(zv.y) : double(zv.y));
+    reinterpret_cast<P2*>(p)[j] = o;
+  }
+  if ((n & 1u) && tid == 0) {
+    const uint32_t i = n - 1;
     const double pi = double(p[i]);
     if (xup) x[i] = alpha * pi + x[i];
     p[i] = PT(upd ? beta * pi + double(z[i]) : double(z[i]));
