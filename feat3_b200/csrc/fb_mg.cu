@@ -17,6 +17,7 @@
 //     the norm is reduced inside the kernel that produces the defect and read by the next.
 #include "fb_mg_internal.cuh"
 #include "fb_mf.cuh"
+#include "fb_rest_staged.cuh"
 #include "fb_coarse.cuh"
 
 #include <algorithm>
@@ -668,6 +669,44 @@ static int spmv_L(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* 
   }
 }
 
+// bulk-staged 3D restriction onto a coarse level whose filter is its lattice boundary: tiles of
+// TYC coarse lines per thread group, 2-deep ring, as many CTAs as fit (2 per SM at 129^3)
+template<typename T, int TYC>
+static int launch_rest_staged(fb_mg* m, const Level& L, const T* xf, const EpiRestrict<T>& epi, double* red) {
+  constexpr int NST = 2;
+  const uint32_t Mc1 = L.tr.Mc1, Mf1 = L.tr.Mf1, Wc = Mc1 - 2;
+  MfTile G{};
+  G.M1 = Mc1; G.N = Mc1 - 1;
+  G.G = std::max<uint32_t>(1, 256 / Wc);
+  G.Lt = G.G * TYC;
+  G.tpp = (Wc + G.Lt - 1) / G.Lt;
+  G.ntiles = Wc * G.tpp;
+  G.cap_x = uint32_t(((uint64_t(2 * G.Lt + 1) * Mf1 * sizeof(T) + 15) & ~uint64_t(15)) + 32);
+  G.stage_bytes = (3 * G.cap_x + 127) & ~127u;
+  G.nbl_items = (4 * Mc1 - 4) * ((Mc1 + 31) / 32);
+  G.nedge_items = (Wc * Wc + 15) / 16;
+  G.direct_masked = 1;
+  const size_t dyn = size_t(NST) * G.stage_bytes;
+  auto fn = k_rest_q1_staged<T, NST, TYC>;
+  static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
+  if (dyn > attr) {
+    FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+    attr = dyn;
+  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, 288, dyn) != cudaSuccess || bps < 1) {
+    cudaGetLastError();
+    bps = 1;
+  }
+  const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(G.ntiles, uint32_t(bps) * kSMs));
+  G.dz = grid / G.tpp;
+  G.dyt = grid % G.tpp;
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(288), dyn, G, Mf1, xf, epi, m->ws, m->counter, red, m->kerr));
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
 // restriction from level l onto level l+1 (R d), epilogue on the coarse rows
 template<typename T, typename Epi>
 static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
@@ -678,6 +717,11 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
         constexpr int CZ = sizeof(T) == 4 ? 4 : 2;  // static shared tile below 48 KB
         // coarse level l+1: its filter is the lattice boundary when structured
         const int bmask = m->L[l + 1].mask_boundary && epi.mask == m->L[l + 1].mask;
+        if (bmask && L.tr.Mc1 >= 65 && L.tr.nf < (1u << 31)) {
+          // FP32 onto 129^3 and up: 4 coarse lines per thread (17 fine lines of a stage); else 2
+          if (sizeof(T) == 4 && L.tr.Mc1 >= 129) return launch_rest_staged<T, 4>(m, L, xf, epi, red);
+          return launch_rest_staged<T, 2>(m, L, xf, epi, red);
+        }
         const uint32_t E = L.tr.Mc1 - (bmask ? 1 : 0);  // indices the grid must cover
         // below 129^3 coarse points, 2 coarse planes per block spread the few blocks better
         // (8.6 vs 12.2 us onto 17^3; 47.8 vs 50.4 us onto 129^3 stays with 4)
