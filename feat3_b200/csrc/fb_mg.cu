@@ -717,10 +717,14 @@ static int rest_T(fb_mg* m, int l, const T* xf, const Epi& epi, double* red) {
         constexpr int CZ = sizeof(T) == 4 ? 4 : 2;  // static shared tile below 48 KB
         // coarse level l+1: its filter is the lattice boundary when structured
         const int bmask = m->L[l + 1].mask_boundary && epi.mask == m->L[l + 1].mask;
-        if (bmask && L.tr.Mc1 >= 65 && L.tr.nf < (1u << 31)) {
-          // FP32 onto 129^3 and up: 4 coarse lines per thread (17 fine lines of a stage); else 2
+        // staged by bulk copies (257^3 solve, same box: 15.97 ms with k_rest_q1_tile on every
+        // level, 15.73 ms staged onto 65^3 and up, 15.62 ms staged onto 17^3 and up); coarse
+        // lines per thread: FP32 onto 129^3 and up 4 (17 fine lines of a stage), 2 onto 65^3
+        // and up, 1 below (more tiles for the CTAs)
+        if (bmask && L.tr.Mc1 >= 17 && L.tr.nf < (1u << 31)) {
           if (sizeof(T) == 4 && L.tr.Mc1 >= 129) return launch_rest_staged<T, 4>(m, L, xf, epi, red);
-          return launch_rest_staged<T, 2>(m, L, xf, epi, red);
+          if (L.tr.Mc1 >= 65) return launch_rest_staged<T, 2>(m, L, xf, epi, red);
+          return launch_rest_staged<T, 1>(m, L, xf, epi, red);
         }
         const uint32_t E = L.tr.Mc1 - (bmask ? 1 : 0);  // indices the grid must cover
         // below 129^3 coarse points, 2 coarse planes per block spread the few blocks better
