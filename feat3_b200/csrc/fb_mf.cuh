@@ -24,6 +24,8 @@
 #pragma once
 #include "fb_sell.cuh"
 
+#include <type_traits>
+
 namespace fb {
 
 // ------------------------------------------------------------------ staged epilogues
@@ -409,71 +411,81 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
         // per cell line: sums of k over the cells selected by (dz, dx) in {-1,0,1}^2
         T K[2][3][3];
         ksums(kw, 0, K[0]);
+        // FAST: every line of the group lies in the tile, the coefficients are given, no filter
+        // word is staged and the smoother runs: rows without a branch, so the loads of a row
+        // can be scheduled ahead of the previous row's epilogue
+        auto rows = [&](auto fast) {
+          constexpr bool FAST = decltype(fast)::value;
 #pragma unroll
-        for (int j = 0; j < TY; ++j) {
-          if (l0 + j >= g.lt) break;
+          for (int j = 0; j < TY; ++j) {
+            if (!FAST && l0 + j >= g.lt) break;
 #pragma unroll
-          for (int q = 0; q < 3; ++q)
+            for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) xw[q][2][d] = T(xs[q][(j + 2) * int(M1) + d - 1]);
-          if (A.k) {
+              for (int d = 0; d < 3; ++d) xw[q][2][d] = T(xs[q][(j + 2) * int(M1) + d - 1]);
+            if (FAST || A.k) {
+#pragma unroll
+              for (int q = 0; q < 2; ++q) {
+                kw[q][1][0] = ks[q][(j + 1) * N];
+                kw[q][1][1] = ks[q][(j + 1) * N + 1];
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < 2; ++q) kw[q][1][0] = kw[q][1][1] = T(1);
+            }
+            // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
+            // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
+            // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b]). The 6 face
+            // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
+            // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
+            ksums(kw, 1, K[1]);
+            T S[8];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) S[r] = T(0);
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+              for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx) {
+                  const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
+                  if (r == 1 || r == 2 || r == 4) continue;
+                  const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
+                  S[r] += Kd * xw[dz][dy][dx];
+                }
+            T s = A.kr[0] * S[0];
+#pragma unroll
+            for (int r = 3; r < 8; ++r)
+              if (r != 4) s += A.kr[r] * S[r];
+            const uint32_t row = r0 + (l0 + j) * M1 + X;
+            T sv[NS > 0 ? NS : 1];
+            if (NS > 0) sv[0] = ss[j * int(M1)];
+            if (NS > 1)
+              sv[NS > 1 ? 1 : 0] =
+                  reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[j * int(M1)];
+            const bool mb = (!FAST && mask) ? ((ms[(row >> 5) - mw0] >> (row & 31)) & 1u) : false;
+            acc += SE::apply(epi, FAST ? false : skp, row, s, xw[1][1][1], sv, mb);
+            // slide the window one line up
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+#pragma unroll
+              for (int d = 0; d < 3; ++d) {
+                xw[q][0][d] = xw[q][1][d];
+                xw[q][1][d] = xw[q][2][d];
+              }
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
-              kw[q][1][0] = ks[q][(j + 1) * N];
-              kw[q][1][1] = ks[q][(j + 1) * N + 1];
-            }
-          } else {
-#pragma unroll
-            for (int q = 0; q < 2; ++q) kw[q][1][0] = kw[q][1][1] = T(1);
-          }
-          // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
-          // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
-          // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b]). The 6 face
-          // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
-          // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
-          ksums(kw, 1, K[1]);
-          T S[8];
-#pragma unroll
-          for (int r = 0; r < 8; ++r) S[r] = T(0);
-#pragma unroll
-          for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-            for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-              for (int dx = 0; dx < 3; ++dx) {
-                const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
-                if (r == 1 || r == 2 || r == 4) continue;
-                const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
-                S[r] += Kd * xw[dz][dy][dx];
-              }
-          T s = A.kr[0] * S[0];
-#pragma unroll
-          for (int r = 3; r < 8; ++r)
-            if (r != 4) s += A.kr[r] * S[r];
-          const uint32_t row = r0 + (l0 + j) * M1 + X;
-          T sv[NS > 0 ? NS : 1];
-          if (NS > 0) sv[0] = ss[j * int(M1)];
-          if (NS > 1) sv[NS > 1 ? 1 : 0] = reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[j * int(M1)];
-          const bool mb = mask ? ((ms[(row >> 5) - mw0] >> (row & 31)) & 1u) : false;
-          acc += SE::apply(epi, skp, row, s, xw[1][1][1], sv, mb);
-          // slide the window one line up
-#pragma unroll
-          for (int q = 0; q < 3; ++q)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              xw[q][0][d] = xw[q][1][d];
-              xw[q][1][d] = xw[q][2][d];
+              kw[q][0][0] = kw[q][1][0];
+              kw[q][0][1] = kw[q][1][1];
             }
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            kw[q][0][0] = kw[q][1][0];
-            kw[q][0][1] = kw[q][1][1];
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int b = 0; b < 3; ++b) K[0][a][b] = K[1][a][b];
           }
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) K[0][a][b] = K[1][a][b];
-        }
+        };
+        if (!skp && !mask && A.k && l0 + TY <= g.lt) rows(std::true_type{});
+        else rows(std::false_type{});
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
