@@ -749,13 +749,8 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
   const uint32_t ly0 = (Y >> 1) - cy0, ly1 = ((Y + 1) >> 1) - cy0;
   const T hx = (X & 1) ? T(0.5) : T(1), hy = (Y & 1) ? T(0.5) : T(1);
   const T wy1 = (Y & 1) ? T(1) : T(0);
-#pragma unroll
-  for (int z = 0; z < FZ; ++z) {
-    if (Z0 + z >= g.Mf1) break;
-    const size_t i = i0 + z * plane;
-    bool msk;
-    if (bmask) msk = bxy || Z0 + z == 0 || Z0 + z == g.Mf1 - 1;
-    else msk = mask ? ((__ldg(mask + (i >> 5)) >> (i & 31)) & 1u) : false;
+  // the correction of plane z of the slab
+  auto corr = [&](int z) {
     const T w = hx * hy * ((z & 1) ? T(0.5) : T(1));
     const T wx1 = (X & 1) ? w : T(0);
     const T wz1 = (z & 1) ? T(1) : T(0);
@@ -769,6 +764,23 @@ __global__ void __launch_bounds__(256) k_prol_q1_tile(Q1Transfer g, const T* __r
     s += (wz1 * wx1) * cm[q1][ly0][lx1];
     s += (wz1 * wy1 * w) * cm[q1][ly1][lx0];
     s += (wz1 * wy1 * wx1) * cm[q1][ly1][lx1];
+    return s;
+  };
+  if (bmask && Z0 > 0 && Z0 + FZ < g.Mf1) {
+    // every plane of the slab is interior: the filter is the column's own test, no branch per row
+    if (bxy) return;
+#pragma unroll
+    for (int z = 0; z < FZ; ++z) sol[i0 + z * plane] = T(1) * corr(z) + old[z];
+    return;
+  }
+#pragma unroll
+  for (int z = 0; z < FZ; ++z) {
+    if (Z0 + z >= g.Mf1) break;
+    const size_t i = i0 + z * plane;
+    bool msk;
+    if (bmask) msk = bxy || Z0 + z == 0 || Z0 + z == g.Mf1 - 1;
+    else msk = mask ? ((__ldg(mask + (i >> 5)) >> (i & 31)) & 1u) : false;
+    const T s = corr(z);
     if (!msk) sol[i] = T(1) * s + old[z];
   }
 }
