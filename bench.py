@@ -32,7 +32,8 @@ METRIC = "time-to-rel-1e-8 (mixed vs FP64 MG-PCG, 1 B200); SpMV HBM GB/s vs 8 TB
 # headline form: FP64 outer PCG around an FP32 V-cycle on the matrix-free operator
 HEAD_PREC, HEAD_FMT = "f32", "matfree"
 HEAD_KERNEL = "matfree_jacobi_f32"
-HEAD_KERNEL_NAME = "k_mf_q1_tiled<float, EpiJacobi<float,0>> finest level (matrix-free Q1, bulk-copy staged)"
+HEAD_KERNEL_NAME = ("k_mf_q1_tiled<float, EpiJacobiK<float,0,0>> finest level (matrix-free Q1, bulk-copy staged, "
+                    "inverse diagonal from the cell coefficients)")
 
 
 def profiled_traffic(kernel):
@@ -327,6 +328,8 @@ def native_arm(args):
         _lib.call("fb_mg_time_spmv", mg.h, 0, which, {"f64": 0, "f32": 1, "f16": 2}[prec], 20, C.byref(ms))
         sx = 8 if prec == "f64" else 4                    # vector element size
         vec = n * sx * (3 if which == 0 else 1)           # Jacobi: rhs, invd, out; PCG q: q (p is the input)
+        if which == 0 and fmt == "matfree" and prec == "f32":
+            vec = n * sx * 2                              # the FP32 tiled step forms invd from the coefficients
         if which == 3:                                    # FP32 direction in, FP64 q out, FP64 coefficients
             vec = n * 8
         if fmt == "matfree":

@@ -42,7 +42,8 @@ struct Staged<EpiJacobi<T, RED, DOT>> {
   static bool input_is_x(const E& e, const void* x) { return e.x == x; }
   static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E& e) { return smoother_skip<T>(e.skip_src); }
-  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st, bool m) {
+  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st, bool m,
+                                                 T) {
     if (skp) {
       const T o = e.s0 ? e.s0[row] : T(0);
       e.out[row] = o;
@@ -60,6 +61,34 @@ struct Staged<EpiJacobi<T, RED, DOT>> {
   }
 };
 
+template<typename T, bool RED, bool DOT>
+struct Staged<EpiJacobiK<T, RED, DOT>> {
+  using E = EpiJacobiK<T, RED, DOT>;
+  static constexpr bool kOk = true;
+  static constexpr int kStreams = 1;
+  static const void* stream(const E& e, int) { return e.rhs; }
+  static bool input_is_x(const E& e, const void* x) { return e.x == x; }
+  static const uint32_t* mask(const E& e) { return e.mask; }
+  __device__ static bool skip(const E& e) { return smoother_skip<T>(e.skip_src); }
+  __device__ __forceinline__ static double apply(const E& e, bool skp, uint32_t row, T s, T xc, const T* st, bool m,
+                                                 T kc) {
+    if (skp) {
+      const T o = e.s0 ? e.s0[row] : T(0);
+      e.out[row] = o;
+      return DOT ? double(o) * double(st[0]) : 0.0;
+    }
+    const T d = st[0] - s;
+    if (m) {
+      e.out[row] = xc;
+      return DOT ? double(xc) * double(st[0]) : 0.0;
+    }
+    const T t = __fdividef(e.wd, kc) * d;
+    const T o = e.omega * t + xc;
+    e.out[row] = o;
+    return RED ? double(d) * double(d) : (DOT ? double(o) * double(st[0]) : 0.0);
+  }
+};
+
 template<typename T, bool RED, bool LOW>
 struct Staged<EpiDefect<T, RED, LOW>> {
   using E = EpiDefect<T, RED, LOW>;
@@ -69,7 +98,7 @@ struct Staged<EpiDefect<T, RED, LOW>> {
   static bool input_is_x(const E&, const void*) { return true; }
   static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E&) { return false; }
-  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T, const T* st, bool m) {
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T, const T* st, bool m, T) {
     T d = st[0] - s;
     if (m) d = T(0);
     e.def[row] = d;
@@ -87,7 +116,7 @@ struct Staged<EpiPcgQ<T, PT>> {
   static bool input_is_x(const E& e, const void* x) { return e.p == x; }  // q . p with p the product's input
   static const uint32_t* mask(const E& e) { return e.mask; }
   __device__ static bool skip(const E&) { return false; }
-  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T xc, const T*, bool m) {
+  __device__ __forceinline__ static double apply(const E& e, bool, uint32_t row, T s, T xc, const T*, bool m, T) {
     const T v = m ? T(0) : s;
     e.q[row] = v;
     return double(v) * double(xc);
@@ -439,6 +468,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
             // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
             // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
             ksums(kw, 1, K[1]);
+            const T kc = K[0][1][1] + K[1][1][1];  // the row's 8 cells
             T S[8];
 #pragma unroll
             for (int r = 0; r < 8; ++r) S[r] = T(0);
@@ -464,7 +494,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
               sv[NS > 1 ? 1 : 0] =
                   reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[j * int(M1)];
             const bool mb = (!FAST && mask) ? ((ms[(row >> 5) - mw0] >> (row & 31)) & 1u) : false;
-            acc += SE::apply(epi, FAST ? false : skp, row, s, xw[1][1][1], sv, mb);
+            acc += SE::apply(epi, FAST ? false : skp, row, s, xw[1][1][1], sv, mb, kc);
             // slide the window one line up
 #pragma unroll
             for (int q = 0; q < 3; ++q)

@@ -586,15 +586,24 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
   constexpr int TY = sizeof(T) == 4 ? 6
                      : std::is_same<Epi, EpiPcgQ<double, float>>::value ? 6
                      : std::is_same<Epi, EpiPcgQ<double>>::value ? 3 : 2;
-  // the FP32 defect streams one vector: 8 lines fit one CTA per SM and ran faster at 257^3
-  // (65.6 us against 71.3 us with 6 lines at two CTAs)
-  constexpr int TY8 = std::is_same<Epi, EpiDefect<float, false, false>>::value ? 8 : TY;
+  // at 257^3: the FP32 defect streams one vector, 8 lines fit one CTA per SM and ran faster
+  // (65.6 us against 71.3 us with 6 lines at two CTAs); the FP32 Jacobi step with the diagonal
+  // from the coefficients streams one vector too, 7 lines still fit two CTAs per SM (solve
+  // 15.05 ms against 15.17 ms with 6 lines, same box)
+  constexpr int TY8 = std::is_same<Epi, EpiDefect<float, false, false>>::value ? 8
+                      : (std::is_same<Epi, EpiJacobiK<float, false, false>>::value ||
+                         std::is_same<Epi, EpiJacobiK<float, true, false>>::value ||
+                         std::is_same<Epi, EpiJacobiK<float, false, true>>::value) ? 7 : TY;
   if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY8, 2, 2, 257, XT>(m, L, v, x, epi, red_out);
   if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129, XT>(m, L, v, x, epi, red_out);
   // the smaller levels have few lines per plane: short tiles spread them over more CTAs
   constexpr int TYS = sizeof(T) == 4 ? 2 : TY;
   return launch_mf_tiled_ty<T, Epi, TYS, 2, 2, 0, XT>(m, L, v, x, epi, red_out);
 }
+
+// the FP32 Jacobi step whose tiled form takes its inverse diagonal from the cell coefficients
+template<typename Epi> struct JacobiK { using type = void; };
+template<bool RED, bool DOT> struct JacobiK<EpiJacobi<float, RED, DOT>> { using type = EpiJacobiK<float, RED, DOT>; };
 
 template<typename T, typename Epi, int DIM>
 static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* red_out) {
@@ -611,8 +620,22 @@ static int launch_mf_D(fb_mg* m, const Level& L, const T* x, const Epi& epi, dou
   for (int j = 0; j < (DIM == 3 ? 27 : 9); ++j) v.off[j] = L.St.off[j];
   if constexpr (DIM == 3 && Staged<Epi>::kOk) {
     if (L.M1 >= 18 && L.n < (1u << 31) && Staged<Epi>::input_is_x(epi, x) && !v.err && m->mf_faces0 &&
-        !(m->cfg.flags & FB_FLAG_NO_TILED))
+        !(m->cfg.flags & FB_FLAG_NO_TILED)) {
+      using EK = typename JacobiK<Epi>::type;
+      if constexpr (!std::is_void<EK>::value) {
+        // the level's stored inverse diagonal is omega_jac / (kr[0] * sum of the row's 8 k):
+        // formed in the kernel, one streamed vector less (solve 15.17 ms against 15.23 ms with
+        // the stored one at 6 lines, same box; the FP32 V-cycle is the preconditioner, and
+        // __fdividef's few-ulp quotient leaves the iteration count unchanged)
+        if (epi.invd == L.invd32) {
+          EK ek;
+          static_cast<Epi&>(ek) = epi;
+          ek.wd = float(m->cfg.omega_jac) / v.kr[0];
+          return launch_mf_tiled<T, EK>(m, L, v, x, ek, red_out);
+        }
+      }
       return launch_mf_tiled<T, Epi>(m, L, v, x, epi, red_out);
+    }
   }
   auto fn = k_mf_q1<T, Epi, DIM>;
   if (debug_enabled())

@@ -119,6 +119,15 @@ struct EpiJacobi {
   }
 };
 
+// The same step for the matrix-free tiled kernel on a Q1 lattice, which forms the inverse
+// diagonal of a tile row from the cell coefficients it already holds: a_vv = kr[0] * (sum of
+// k over the row's 8 cells), so invd = wd / sum with wd = omega_jac / kr[0] (one streamed
+// vector less). Rows outside the tiles use the stored invd.
+template<typename T, bool RED = false, bool DOT = false>
+struct EpiJacobiK : EpiJacobi<T, RED, DOT> {
+  T wd;
+};
+
 // PCG direction product: q = filter_def(A p), reduction q . p
 // (p may be stored in FP32 when the outer solver keeps its search direction in FP32; the product
 // and q stay in T)
