@@ -259,6 +259,17 @@ __device__ __forceinline__ void ksums(const T (&kw)[2][2][2], int c, T (&K)[3][3
   K[1][1] = K[0][1] + K[2][1];
 }
 
+// the same sums with the two cell planes packed: kp[ex] = (k of plane Z-1, k of plane Z) for
+// cell columns ex = 0, 1 of one cell line; Kp[dx] = (K[0][dx], K[2][dx]), Km[dx] = K[1][dx]
+__device__ __forceinline__ void ksums2(const float2 (&kp)[2], float2 (&Kp)[3], float (&Km)[3]) {
+  Kp[0] = kp[0];
+  Kp[2] = kp[1];
+  Kp[1] = __fadd2_rn(kp[0], kp[1]);
+  Km[0] = kp[0].x + kp[0].y;
+  Km[2] = kp[1].x + kp[1].y;
+  Km[1] = Kp[1].x + Kp[1].y;
+}
+
 // ------------------------------------------------------------------ the tiled kernel
 // 8 consumer warps + 1 producer warp; dynamic shared memory = NST * G.stage_bytes.
 // CM1: the lattice size as a compile-time constant (0: G.M1 at run time), which turns the
@@ -274,6 +285,8 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
   constexpr int NS = SE::kStreams;
   constexpr uint64_t E = 16 / sizeof(T);
   constexpr uint64_t EX = 16 / sizeof(XT);
+  // FP32 throughout: the stencil runs on packed FP32 pairs (fma.rn.f32x2)
+  constexpr bool PK = std::is_same<T, float>::value && std::is_same<XT, float>::value;
   pdl_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[NST], empty[NST];
@@ -424,22 +437,39 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
         const T* ss = reinterpret_cast<const T*>(st + off_s) + (r0 & uint32_t(E - 1)) + l0 * M1 + X;
         const uint32_t* ms = reinterpret_cast<const uint32_t*>(st + off_m);
         const uint32_t mw0 = (r0 >> 5) & ~3u;  // first staged mask word
-        // window: xw[plane][line][dx], kw[cell plane][cell line][ex]
+        // window: xw[plane][line][dx], kw[cell plane][cell line][ex]; in the packed FP32 form
+        // xp[line][dx] pairs planes Z-1 and Z+1, xm[line][dx] is plane Z, kp[cell line][ex]
+        // pairs cell planes Z-1 and Z (the unused form's arrays are dead code)
         T xw[3][3][3], kw[2][2][2];
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
+        float2 xp[3][3], kp[2][2], Kp[2][3];
+        T xm[3][3], Km[2][3];
+        // per cell line: sums of k over the cells selected by (dz, dx) in {-1,0,1}^2
+        T K[2][3][3];
+        if constexpr (PK) {
 #pragma unroll
           for (int l = 0; l < 2; ++l)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) xw[q][l][d] = T(xs[q][l * int(M1) + d - 1]);
+            for (int d = 0; d < 3; ++d) {
+              xp[l][d] = make_float2(xs[0][l * int(M1) + d - 1], xs[2][l * int(M1) + d - 1]);
+              xm[l][d] = xs[1][l * int(M1) + d - 1];
+            }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          kw[q][0][0] = A.k ? ks[q][0] : T(1);
-          kw[q][0][1] = A.k ? ks[q][1] : T(1);
+          for (int c = 0; c < 2; ++c) kp[0][c] = A.k ? make_float2(ks[0][c], ks[1][c]) : make_float2(1.f, 1.f);
+          ksums2(kp[0], Kp[0], Km[0]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int l = 0; l < 2; ++l)
+#pragma unroll
+              for (int d = 0; d < 3; ++d) xw[q][l][d] = T(xs[q][l * int(M1) + d - 1]);
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            kw[q][0][0] = A.k ? ks[q][0] : T(1);
+            kw[q][0][1] = A.k ? ks[q][1] : T(1);
+          }
+          ksums(kw, 0, K[0]);
         }
-        // per cell line: sums of k over the cells selected by (dz, dx) in {-1,0,1}^2
-        T K[2][3][3];
-        ksums(kw, 0, K[0]);
         // FAST: every line of the group lies in the tile, the coefficients are given, no filter
         // word is staged and the smoother runs: rows without a branch, so the loads of a row
         // can be scheduled ahead of the previous row's epilogue
@@ -448,45 +478,85 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
 #pragma unroll
           for (int j = 0; j < TY; ++j) {
             if (!FAST && l0 + j >= g.lt) break;
+            T s, kc, xc;
+            if constexpr (PK) {
+              // packed FP32 form: the neighbours in planes Z-1 and Z+1 pair up (same line and
+              // column, lanes x and y), two FP32 operations per instruction; the terms are those
+              // of the scalar form, summed plane pair by plane pair
 #pragma unroll
-            for (int q = 0; q < 3; ++q)
-#pragma unroll
-              for (int d = 0; d < 3; ++d) xw[q][2][d] = T(xs[q][(j + 2) * int(M1) + d - 1]);
-            if (FAST || A.k) {
-#pragma unroll
-              for (int q = 0; q < 2; ++q) {
-                kw[q][1][0] = ks[q][(j + 1) * N];
-                kw[q][1][1] = ks[q][(j + 1) * N + 1];
+              for (int d = 0; d < 3; ++d) {
+                xp[2][d] = make_float2(xs[0][(j + 2) * int(M1) + d - 1], xs[2][(j + 2) * int(M1) + d - 1]);
+                xm[2][d] = xs[1][(j + 2) * int(M1) + d - 1];
               }
+#pragma unroll
+              for (int c = 0; c < 2; ++c)
+                kp[1][c] = (FAST || A.k) ? make_float2(ks[0][(j + 1) * N + c], ks[1][(j + 1) * N + c])
+                                         : make_float2(1.f, 1.f);
+              ksums2(kp[1], Kp[1], Km[1]);
+              kc = Km[0][1] + Km[1][1];  // the row's 8 cells
+              // r = 5 (dx != 1, dy = 1), 6 (dx = 1, dy != 1), 7 (dx, dy != 1), planes Z-1 / Z+1
+              float2 S5 = __fmul2_rn(__fadd2_rn(Kp[0][0], Kp[1][0]), xp[1][0]);
+              S5 = __ffma2_rn(__fadd2_rn(Kp[0][2], Kp[1][2]), xp[1][2], S5);
+              float2 S6 = __fmul2_rn(Kp[0][1], xp[0][1]);
+              S6 = __ffma2_rn(Kp[1][1], xp[2][1], S6);
+              float2 S7 = __fmul2_rn(Kp[0][0], xp[0][0]);
+              S7 = __ffma2_rn(Kp[0][2], xp[0][2], S7);
+              S7 = __ffma2_rn(Kp[1][0], xp[2][0], S7);
+              S7 = __ffma2_rn(Kp[1][2], xp[2][2], S7);
+              // plane Z: the centre (r = 0) and r = 3 (dx, dy != 1)
+              const T S0 = kc * xm[1][1];
+              T S3 = Km[0][0] * xm[0][0];
+              S3 += Km[0][2] * xm[0][2];
+              S3 += Km[1][0] * xm[2][0];
+              S3 += Km[1][2] * xm[2][2];
+              s = A.kr[0] * S0;
+              s += A.kr[3] * S3;
+              s += A.kr[5] * (S5.x + S5.y);
+              s += A.kr[6] * (S6.x + S6.y);
+              s += A.kr[7] * (S7.x + S7.y);
+              xc = xm[1][1];
             } else {
 #pragma unroll
-              for (int q = 0; q < 2; ++q) kw[q][1][0] = kw[q][1][1] = T(1);
-            }
-            // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
-            // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
-            // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b]). The 6 face
-            // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
-            // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
-            ksums(kw, 1, K[1]);
-            const T kc = K[0][1][1] + K[1][1][1];  // the row's 8 cells
-            T S[8];
+              for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int r = 0; r < 8; ++r) S[r] = T(0);
+                for (int d = 0; d < 3; ++d) xw[q][2][d] = T(xs[q][(j + 2) * int(M1) + d - 1]);
+              if (FAST || A.k) {
 #pragma unroll
-            for (int dz = 0; dz < 3; ++dz)
-#pragma unroll
-              for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-                for (int dx = 0; dx < 3; ++dx) {
-                  const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
-                  if (r == 1 || r == 2 || r == 4) continue;
-                  const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
-                  S[r] += Kd * xw[dz][dy][dx];
+                for (int q = 0; q < 2; ++q) {
+                  kw[q][1][0] = ks[q][(j + 1) * N];
+                  kw[q][1][1] = ks[q][(j + 1) * N + 1];
                 }
-            T s = A.kr[0] * S[0];
+              } else {
 #pragma unroll
-            for (int r = 3; r < 8; ++r)
-              if (r != 4) s += A.kr[r] * S[r];
+                for (int q = 0; q < 2; ++q) kw[q][1][0] = kw[q][1][1] = T(1);
+              }
+              // stencil form of the cell sum: the coefficient of neighbour d is kr[r(d)] times the
+              // sum of k over the cells holding both the row's node and d, where r(d) has a bit for
+              // every direction in which d is nonzero (K_ref[a][b] = kr[a ^ b]). The 6 face
+              // neighbours (one bit in r) have coefficient 0 for the Q1 Laplacian of a cube (the
+              // launcher checks kr[1], kr[2], kr[4] are of rounding size) and are left out.
+              ksums(kw, 1, K[1]);
+              kc = K[0][1][1] + K[1][1][1];  // the row's 8 cells
+              T S[8];
+#pragma unroll
+              for (int r = 0; r < 8; ++r) S[r] = T(0);
+#pragma unroll
+              for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+                  for (int dx = 0; dx < 3; ++dx) {
+                    const int r = (dx != 1 ? 1 : 0) | (dy != 1 ? 2 : 0) | (dz != 1 ? 4 : 0);
+                    if (r == 1 || r == 2 || r == 4) continue;
+                    const T Kd = dy == 0 ? K[0][dz][dx] : (dy == 2 ? K[1][dz][dx] : K[0][dz][dx] + K[1][dz][dx]);
+                    S[r] += Kd * xw[dz][dy][dx];
+                  }
+              s = A.kr[0] * S[0];
+#pragma unroll
+              for (int r = 3; r < 8; ++r)
+                if (r != 4) s += A.kr[r] * S[r];
+              xc = xw[1][1][1];
+            }
             const uint32_t row = r0 + (l0 + j) * M1 + X;
             T sv[NS > 0 ? NS : 1];
             if (NS > 0) sv[0] = ss[j * int(M1)];
@@ -494,24 +564,38 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
               sv[NS > 1 ? 1 : 0] =
                   reinterpret_cast<const T*>(reinterpret_cast<const unsigned char*>(ss) + G.cap_s)[j * int(M1)];
             const bool mb = (!FAST && mask) ? ((ms[(row >> 5) - mw0] >> (row & 31)) & 1u) : false;
-            acc += SE::apply(epi, FAST ? false : skp, row, s, xw[1][1][1], sv, mb, kc);
+            acc += SE::apply(epi, FAST ? false : skp, row, s, xc, sv, mb, kc);
             // slide the window one line up
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
+            if constexpr (PK) {
 #pragma unroll
               for (int d = 0; d < 3; ++d) {
-                xw[q][0][d] = xw[q][1][d];
-                xw[q][1][d] = xw[q][2][d];
+                xp[0][d] = xp[1][d];
+                xp[1][d] = xp[2][d];
+                xm[0][d] = xm[1][d];
+                xm[1][d] = xm[2][d];
+                Kp[0][d] = Kp[1][d];
+                Km[0][d] = Km[1][d];
+              }
+              kp[0][0] = kp[1][0];
+              kp[0][1] = kp[1][1];
+            } else {
+#pragma unroll
+              for (int q = 0; q < 3; ++q)
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                  xw[q][0][d] = xw[q][1][d];
+                  xw[q][1][d] = xw[q][2][d];
+                }
+#pragma unroll
+              for (int q = 0; q < 2; ++q) {
+                kw[q][0][0] = kw[q][1][0];
+                kw[q][0][1] = kw[q][1][1];
               }
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-              kw[q][0][0] = kw[q][1][0];
-              kw[q][0][1] = kw[q][1][1];
+              for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int b = 0; b < 3; ++b) K[0][a][b] = K[1][a][b];
             }
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int b = 0; b < 3; ++b) K[0][a][b] = K[1][a][b];
           }
         };
         if (!skp && !mask && A.k && l0 + TY <= g.lt) rows(std::true_type{});
