@@ -153,15 +153,19 @@ def test_zero_rhs_and_nan_status():
     assert r["status"] == "aborted"
 
 
+@pytest.mark.parametrize("lvl", [4, 5, 6])
 @pytest.mark.parametrize("fmt", ["sell", "stencil", "matfree"])
-def test_vcycle_matches_oracle(fmt):
+def test_vcycle_matches_oracle(fmt, lvl):
+    """one V(2,2) cycle against the oracle's; from level 5 on the restriction onto the 17^3 and
+    33^3 levels runs as the bulk-staged kernel, whose terms and order are those of R"""
     from feat3_b200.solver import MultiGrid
-    H = po.Hierarchy(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11))
+    H = po.Hierarchy(3, 1, lvl, 1, lognormal_k(3, lvl, 1.0, 11))
     d = H.rhs("one")
     ref = H.vcycle(d, nu=2)
-    mg = MultiGrid.structured(3, 1, 4, 1, lognormal_k(3, 4, 1.0, 11)).configure(nu=2, format=fmt)
+    mg = MultiGrid.structured(3, 1, lvl, 1, lognormal_k(3, lvl, 1.0, 11)).configure(nu=2, format=fmt)
     cor = mg.vcycle(torch.tensor(d).cuda()).cpu().numpy()
     assert relerr(cor, ref) <= 1e-13
+    mg.close()
 
 
 def test_adjoint_gradient_matches_oracle():
