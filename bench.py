@@ -33,7 +33,7 @@ METRIC = "time-to-rel-1e-8 (mixed vs FP64 MG-PCG, 1 B200); SpMV HBM GB/s vs 8 TB
 HEAD_PREC, HEAD_FMT = "f32", "matfree"
 HEAD_KERNEL = "matfree_jacobi_f32"
 HEAD_KERNEL_NAME = ("k_mf_q1_tiled<float, EpiJacobiK<float,0,0>> finest level (matrix-free Q1, bulk-copy staged, "
-                    "inverse diagonal from the cell coefficients)")
+                    "inverse diagonal from the cell coefficients, packed FP32 pairs)")
 
 
 def profiled_traffic(kernel):
