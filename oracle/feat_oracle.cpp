@@ -1,6 +1,10 @@
 // CPU oracle (TEST INFRASTRUCTURE ONLY) -- see feat_oracle.h for scope and citations.
-// Plain serial C++: every loop follows the reference's summation order where the
-// reference defines one (CSR row sums, sequential dot products).
+// Plain C++: every loop follows the reference's summation order where the reference
+// defines one (CSR row sums, sequential dot products). Loops whose iterations are
+// independent (rows of a matrix product, entries of a vector update, rows of the
+// assembled matrices, elements) run on OpenMP threads; each iteration computes exactly
+// what the serial loop computes, so results do not depend on the thread count. The
+// reductions (dot, norm2) stay sequential, in the reference's order.
 #include "feat_oracle.h"
 
 #include <algorithm>
@@ -15,6 +19,9 @@
 namespace {
 
 template<typename T> T eps() { return std::numeric_limits<T>::epsilon(); }
+
+// loops shorter than this stay on the calling thread (the coarse levels)
+constexpr int64_t kParMin = 1 << 15;
 
 // ------------------------------------------------------------------------------------
 // 1D reference-element data, Gauss-Legendre 3 points on [-1,1] (auto-degree:5 ->
@@ -52,15 +59,18 @@ struct CSR {
 template<typename T>
 void csr_apply(T* r, T a, const T* x, T b, const T* y, const CSR<T>& A) {
   const int64_t n = A.rows;
-  if (std::fabs(b) < eps<T>()) {
-    for (int64_t i = 0; i < n; ++i) r[i] = T(0);
-  } else if (r != y) {
-    for (int64_t i = 0; i < n; ++i) r[i] = y[i];
-  }
+  const bool zero = std::fabs(b) < eps<T>();
+  const int64_t* rp = A.rp.data();
+  const int32_t* ci = A.ci.data();
+  const T* va = A.va.data();
+#pragma omp parallel for schedule(static) if (n >= kParMin)
   for (int64_t row = 0; row < n; ++row) {
+    // r is zeroed (|b| < eps) or set to y before the product, row by row as the reference
+    // does array-wide; each row reads only its own r entry
+    const T rr = zero ? T(0) : y[row];
     T sum(0);
-    for (int64_t k = A.rp[row]; k < A.rp[row + 1]; ++k) sum += A.va[k] * x[A.ci[k]];
-    r[row] = (sum * a) + (b * r[row]);
+    for (int64_t k = rp[row]; k < rp[row + 1]; ++k) sum += va[k] * x[ci[k]];
+    r[row] = (sum * a) + (b * rr);
   }
 }
 
@@ -80,11 +90,24 @@ T norm2(const T* x, int64_t n) {  // norm_generic.hpp:24-32
 template<typename T>
 void axpy(T* r, const T* x, const T* y, T alpha, int64_t n) {
   if (std::fabs(alpha) < eps<T>()) {
-    if (r != y) for (int64_t i = 0; i < n; ++i) r[i] = y[i];
+    if (r != y) {
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+      for (int64_t i = 0; i < n; ++i) r[i] = y[i];
+    }
     return;
   }
+#pragma omp parallel for schedule(static) if (n >= kParMin)
   for (int64_t i = 0; i < n; ++i) r[i] = alpha * x[i] + y[i];
 }
+
+template<typename T, typename U>
+void convert(T* dst, const U* src, int64_t n) {
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) dst[i] = T(src[i]);
+}
+
+template<typename T>
+void copy_vec(T* dst, const T* src, int64_t n) { convert(dst, src, n); }
 
 // ------------------------------------------------------------------------------------
 // structured level
@@ -159,56 +182,91 @@ inline int64_t elem_dof(const or_hier& H, const LevelD& L, int64_t e, int a) {
   return X + M1 * (Y + M1 * Z);
 }
 
+// elements containing lattice coordinate X along one direction (element ex spans the lattice
+// points [p*ex, p*ex + p]) and the lattice range their dofs cover
+struct Span1 { int64_t e0, e1, c0, c1; };
+inline Span1 span1(int64_t X, int p, int64_t N) {
+  Span1 s;
+  s.e0 = std::max<int64_t>(0, (X + p - 1) / p - 1);
+  s.e1 = std::min<int64_t>(N - 1, X / p);
+  s.c0 = int64_t(p) * s.e0;
+  s.c1 = int64_t(p) * s.e1 + p;
+  return s;
+}
+
+// Assembly of the structured level (bilinear_operator_assembler.hpp:218-339, pattern of
+// symbolic_assembler.hpp assemble_matrix_std1). The reference scatters k_e*K_e element by
+// element into the CSR rows; here each row gathers the same products from the elements that
+// contain it, in ascending element order, so every entry receives the same terms in the same
+// order as the scatter (bit-identical), with the rows independent of each other. The row's
+// columns are the union of its elements' dofs: per direction a contiguous lattice range, so the
+// row is the tensor product of three ranges and lexicographic order is ascending column order.
 void build_level(or_hier& H, LevelD& L) {
-  const int d = H.dim;
-  const int64_t M1 = L.M + 1;
+  const int d = H.dim, p = H.degree, q1 = p + 1;
+  const int64_t M1 = L.M + 1, N = L.N;
   L.n = 1; L.ne = 1;
-  for (int a = 0; a < d; ++a) { L.n *= M1; L.ne *= L.N; }
+  for (int a = 0; a < d; ++a) { L.n *= M1; L.ne *= N; }
   const int nloc = H.nloc;
-  // pattern: union of element dof sets
-  std::vector<std::vector<int32_t>> adj(L.n);
-  std::vector<int64_t> loc(nloc);
-  for (int64_t e = 0; e < L.ne; ++e) {
-    for (int a = 0; a < nloc; ++a) loc[a] = elem_dof(H, L, e, a);
-    for (int a = 0; a < nloc; ++a)
-      for (int b = 0; b < nloc; ++b) adj[loc[a]].push_back((int32_t)loc[b]);
-  }
+  const int64_t n = L.n;
+  auto coords = [&](int64_t i, int64_t* c) {
+    c[0] = i % M1; c[1] = (i / M1) % M1; c[2] = (d == 3) ? i / (M1 * M1) : 0;
+  };
   CSR<double>& A = L.A;
-  A.rows = A.cols = L.n;
-  A.rp.assign(L.n + 1, 0);
-  for (int64_t i = 0; i < L.n; ++i) {
-    auto& v = adj[i];
-    std::sort(v.begin(), v.end());
-    v.erase(std::unique(v.begin(), v.end()), v.end());
-    A.rp[i + 1] = A.rp[i] + (int64_t)v.size();
+  A.rows = A.cols = n;
+  A.rp.assign(n + 1, 0);
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c[3];
+    coords(i, c);
+    int64_t w = 1;
+    for (int a = 0; a < d; ++a) { const Span1 s = span1(c[a], p, N); w *= s.c1 - s.c0 + 1; }
+    A.rp[i + 1] = w;
   }
-  A.ci.resize(A.rp[L.n]);
-  A.va.assign(A.rp[L.n], 0.0);
-  for (int64_t i = 0; i < L.n; ++i) std::copy(adj[i].begin(), adj[i].end(), A.ci.begin() + A.rp[i]);
-  adj.clear(); adj.shrink_to_fit();
-  // numeric: scatter k_e * scale * K_ref (bilinear_operator_assembler.hpp:218-339)
-  const int lvl = (int)std::lround(std::log2((double)L.N));
+  for (int64_t i = 0; i < n; ++i) A.rp[i + 1] += A.rp[i];
+  A.ci.resize(A.rp[n]);
+  A.va.assign(A.rp[n], 0.0);
+  const int lvl = (int)std::lround(std::log2((double)N));
   const double sc = H.h_scale(lvl);
-  for (int64_t e = 0; e < L.ne; ++e) {
-    const double ke = L.k.empty() ? 1.0 : L.k[e];
-    for (int a = 0; a < nloc; ++a) loc[a] = elem_dof(H, L, e, a);
-    for (int a = 0; a < nloc; ++a) {
-      const int64_t row = loc[a];
-      for (int b = 0; b < nloc; ++b) {
-        const int64_t c = loc[b];
-        auto it = std::lower_bound(A.ci.begin() + A.rp[row], A.ci.begin() + A.rp[row + 1], (int32_t)c);
-        A.va[it - A.ci.begin()] += ke * sc * H.kref1[size_t(a) * nloc + b];
-      }
-    }
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c[3];
+    coords(i, c);
+    Span1 s[3] = {span1(c[0], p, N), span1(c[1], p, N), {0, 0, 0, 0}};
+    s[2] = (d == 3) ? span1(c[2], p, N) : Span1{0, 0, 0, 0};
+    const int64_t wx = s[0].c1 - s[0].c0 + 1, wy = s[1].c1 - s[1].c0 + 1, wz = s[2].c1 - s[2].c0 + 1;
+    int32_t* ci = A.ci.data() + A.rp[i];
+    double* va = A.va.data() + A.rp[i];
+    int64_t pos = 0;
+    for (int64_t z = 0; z < wz; ++z)
+      for (int64_t y = 0; y < wy; ++y)
+        for (int64_t x = 0; x < wx; ++x)
+          ci[pos++] = (int32_t)((s[0].c0 + x) + M1 * ((s[1].c0 + y) + M1 * (s[2].c0 + z)));
+    for (int64_t ez = s[2].e0; ez <= s[2].e1; ++ez)
+      for (int64_t ey = s[1].e0; ey <= s[1].e1; ++ey)
+        for (int64_t ex = s[0].e0; ex <= s[0].e1; ++ex) {
+          const int64_t e = ex + N * (ey + N * ez);
+          const double ke = L.k.empty() ? 1.0 : L.k[e];
+          const int ax = int(c[0] - p * ex), ay = int(c[1] - p * ey), az = int(c[2] - p * ez);
+          const int a = ax + q1 * (ay + q1 * az);
+          for (int b = 0; b < nloc; ++b) {
+            const int bx = b % q1, by = (b / q1) % q1, bz = b / (q1 * q1);
+            const int64_t px = p * ex + bx - s[0].c0, py = p * ey + by - s[1].c0, pz = p * ez + bz - s[2].c0;
+            va[px + wx * (py + wy * pz)] += ke * sc * H.kref1[size_t(a) * nloc + b];
+          }
+        }
   }
   // filter: all lattice points on the boundary
-  L.dir.assign(L.n, 0);
-  for (int64_t i = 0; i < L.n; ++i) {
-    int64_t c[3] = {i % M1, (i / M1) % M1, i / (M1 * M1)};
+  L.dir.assign(n, 0);
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t c[3];
+    coords(i, c);
     bool b = false;
     for (int a = 0; a < d; ++a) b = b || c[a] == 0 || c[a] == L.M;
-    if (b) { L.dir[i] = 1; L.filt.push_back((int32_t)i); }
+    L.dir[i] = b ? 1 : 0;
   }
+  for (int64_t i = 0; i < n; ++i)
+    if (L.dir[i]) L.filt.push_back((int32_t)i);
 }
 
 // nested-space interpolation weights of a coarse 1D basis at fine lattice offsets.
@@ -235,39 +293,53 @@ void prol_1d(int degree, int64_t Mf, std::vector<std::vector<std::pair<int32_t, 
   }
 }
 
+// P row of fine point i: the tensor product of the 1D weight lists (each ascending in the coarse
+// index, so the product taken z, y, x is ascending in the lexicographic column); R = P^T.
 void build_prol(or_hier& H, LevelD& Lf, const LevelD& Lc) {
   const int d = H.dim;
   std::vector<std::vector<std::pair<int32_t, double>>> w;
   prol_1d(H.degree, Lf.M, w);
-  const int64_t Mf1 = Lf.M + 1, Mc1 = Lc.M + 1;
+  const int64_t Mf1 = Lf.M + 1, Mc1 = Lc.M + 1, n = Lf.n;
+  static const std::vector<std::pair<int32_t, double>> one = {{0, 1.0}};
+  auto lists = [&](int64_t i, const std::vector<std::pair<int32_t, double>>** l) {
+    l[0] = &w[i % Mf1];
+    l[1] = &w[(i / Mf1) % Mf1];
+    l[2] = (d == 3) ? &w[i / (Mf1 * Mf1)] : &one;
+  };
   CSR<double>& P = Lf.P;
-  P.rows = Lf.n; P.cols = Lc.n;
-  P.rp.assign(Lf.n + 1, 0);
-  std::vector<std::pair<int32_t, double>> row;
-  for (int64_t i = 0; i < Lf.n; ++i) {
-    int64_t c[3] = {i % Mf1, (i / Mf1) % Mf1, (d == 3) ? i / (Mf1 * Mf1) : 0};
-    row.clear();
-    const auto& wx = w[c[0]];
-    const auto& wy = w[c[1]];
-    static const std::vector<std::pair<int32_t, double>> one = {{0, 1.0}};
-    const auto& wz = (d == 3) ? w[c[2]] : one;
-    for (auto& z : wz)
-      for (auto& y : wy)
-        for (auto& x : wx)
-          row.push_back({(int32_t)(x.first + Mc1 * (y.first + Mc1 * z.first)), x.second * y.second * z.second});
-    std::sort(row.begin(), row.end());
-    for (auto& e : row) { P.ci.push_back(e.first); P.va.push_back(e.second); }
-    P.rp[i + 1] = (int64_t)P.ci.size();
+  P.rows = n; P.cols = Lc.n;
+  P.rp.assign(n + 1, 0);
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) {
+    const std::vector<std::pair<int32_t, double>>* l[3];
+    lists(i, l);
+    P.rp[i + 1] = int64_t(l[0]->size() * l[1]->size() * l[2]->size());
   }
-  // R = P^T (sparse_matrix_csr.hpp transpose)
+  for (int64_t i = 0; i < n; ++i) P.rp[i + 1] += P.rp[i];
+  P.ci.resize(P.rp[n]);
+  P.va.resize(P.rp[n]);
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) {
+    const std::vector<std::pair<int32_t, double>>* l[3];
+    lists(i, l);
+    int64_t k = P.rp[i];
+    for (auto& z : *l[2])
+      for (auto& y : *l[1])
+        for (auto& x : *l[0]) {
+          P.ci[k] = (int32_t)(x.first + Mc1 * (y.first + Mc1 * z.first));
+          P.va[k] = x.second * y.second * z.second;
+          ++k;
+        }
+  }
+  // R = P^T (sparse_matrix_csr.hpp transpose): entries of a coarse row ascending in the fine row
   CSR<double>& R = Lf.R;
-  R.rows = Lc.n; R.cols = Lf.n;
+  R.rows = Lc.n; R.cols = n;
   R.rp.assign(Lc.n + 1, 0);
   for (auto c : P.ci) R.rp[c + 1]++;
   for (int64_t i = 0; i < Lc.n; ++i) R.rp[i + 1] += R.rp[i];
   R.ci.resize(P.ci.size()); R.va.resize(P.va.size());
   std::vector<int64_t> pos(R.rp.begin(), R.rp.end() - 1);
-  for (int64_t i = 0; i < Lf.n; ++i)
+  for (int64_t i = 0; i < n; ++i)
     for (int64_t k = P.rp[i]; k < P.rp[i + 1]; ++k) {
       const int64_t dst = pos[P.ci[k]]++;
       R.ci[dst] = (int32_t)i; R.va[dst] = P.va[k];
@@ -278,7 +350,11 @@ void build_prol(or_hier& H, LevelD& Lf, const LevelD& Lc) {
 // typed multigrid level (FP64 or FP32 inner)
 template<typename T>
 struct MGLevel {
-  CSR<T> A, P, R;
+  // FP64 levels use the hierarchy's matrices; converted (FP32 / FP16-quantised) levels own copies
+  CSR<T> A_own, P_own, R_own;
+  const CSR<T>* A = nullptr;
+  const CSR<T>* P = nullptr;
+  const CSR<T>* R = nullptr;
   std::vector<T> inv_diag;
   const std::vector<int32_t>* filt = nullptr;
   std::vector<T> sol, rhs, def, cor, tmp;
@@ -290,26 +366,48 @@ struct MGLevel {
 };
 
 template<typename T>
-void filter_zero(T* v, const std::vector<int32_t>& f) { for (auto i : f) v[i] = T(0); }
+void filter_zero(T* v, const std::vector<int32_t>& f) {
+  const int64_t n = (int64_t)f.size();
+  const int32_t* idx = f.data();
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) v[idx[i]] = T(0);
+}
 
 template<typename T>
-CSR<T> cast_csr(const CSR<double>& a, int quant) {
-  CSR<T> r;
+void fill_vec(T* v, T x, int64_t n) {
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+  for (int64_t i = 0; i < n; ++i) v[i] = x;
+}
+
+template<typename T>
+void cast_csr(const CSR<double>& a, CSR<T>& r, int quant) {
   r.rows = a.rows; r.cols = a.cols; r.rp = a.rp; r.ci = a.ci;
-  r.va.resize(a.va.size());
+  const int64_t nz = (int64_t)a.va.size();
+  r.va.resize(nz);
   if (quant == 2) {
-    double amax = 0.0;
-    for (double v : a.va) amax = std::max(amax, std::fabs(v));
+    double amax = 0.0;  // max is exact, so the reduction order does not matter
+#pragma omp parallel for schedule(static) reduction(max : amax) if (nz >= kParMin)
+    for (int64_t i = 0; i < nz; ++i) amax = std::max(amax, std::fabs(a.va[i]));
     const double scale = (amax > 0.0) ? amax / 16384.0 : 1.0;
     const double inv = 1.0 / scale;
-    for (size_t i = 0; i < a.va.size(); ++i) {
+#pragma omp parallel for schedule(static) if (nz >= kParMin)
+    for (int64_t i = 0; i < nz; ++i) {
       _Float16 h = (_Float16)(a.va[i] * inv);
       r.va[i] = T(float(h) * float(scale));
     }
   } else {
-    for (size_t i = 0; i < a.va.size(); ++i) r.va[i] = T(a.va[i]);
+    convert(r.va.data(), a.va.data(), nz);
   }
-  return r;
+}
+
+// the level's matrix as the multigrid uses it: the hierarchy's own FP64 matrix, or a converted copy
+template<typename T>
+const CSR<T>* view_or_cast(const CSR<double>& a, CSR<T>& own, int quant) {
+  if constexpr (std::is_same<T, double>::value) {
+    if (quant == 0) return &a;
+  }
+  cast_csr<T>(a, own, quant);
+  return &own;
 }
 
 template<typename T>
@@ -326,30 +424,33 @@ struct MG {
     for (int i = 0; i < nl; ++i) {
       const LevelD& src = h->lv[h->level - i];
       MGLevel<T>& m = L[i];
-      m.A = cast_csr<T>(src.A, quant);
-      if (i + 1 < nl) { m.P = cast_csr<T>(src.P, 0); m.R = cast_csr<T>(src.R, 0); }
+      m.A = view_or_cast(src.A, m.A_own, quant);
+      if (i + 1 < nl) { m.P = view_or_cast(src.P, m.P_own, 0); m.R = view_or_cast(src.R, m.R_own, 0); }
       m.filt = &src.filt;
       const int64_t n = src.n;
       // Jacobi init: extract diag, invert with omega (jacobi_precond.hpp:137-144)
       m.inv_diag.assign(n, T(0));
-      for (int64_t r = 0; r < n; ++r)
-        for (int64_t k = m.A.rp[r]; k < m.A.rp[r + 1]; ++k)
-          if (m.A.ci[k] == r) m.inv_diag[r] = m.A.va[k];
-      for (int64_t r = 0; r < n; ++r) m.inv_diag[r] = T(c.omega_jac) / m.inv_diag[r];
+      const CSR<T>& Am = *m.A;
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+      for (int64_t r = 0; r < n; ++r) {
+        for (int64_t k = Am.rp[r]; k < Am.rp[r + 1]; ++k)
+          if (Am.ci[k] == r) m.inv_diag[r] = Am.va[k];
+        m.inv_diag[r] = T(c.omega_jac) / m.inv_diag[r];
+      }
       m.sol.assign(n, T(0)); m.rhs = m.def = m.cor = m.tmp = m.s_def = m.s_cor = m.sol;
     }
     if (c.coarse == 0) init_direct(L[nl - 1]);
   }
 
   void init_direct(MGLevel<T>& m) {
-    const int64_t n = m.A.rows;
+    const int64_t n = m.A->rows;
     m.lu.assign(size_t(n) * n, 0.0);
     std::vector<char> dir(n, 0);
     for (auto i : *m.filt) dir[i] = 1;
     for (int64_t i = 0; i < n; ++i) {
       if (dir[i]) { m.lu[size_t(i) * n + i] = 1.0; continue; }
-      for (int64_t k = m.A.rp[i]; k < m.A.rp[i + 1]; ++k)
-        if (!dir[m.A.ci[k]]) m.lu[size_t(i) * n + m.A.ci[k]] = double(m.A.va[k]);
+      for (int64_t k = m.A->rp[i]; k < m.A->rp[i + 1]; ++k)
+        if (!dir[m.A->ci[k]]) m.lu[size_t(i) * n + m.A->ci[k]] = double(m.A->va[k]);
     }
     m.piv.resize(n);
     for (int64_t k = 0; k < n; ++k) {
@@ -367,7 +468,7 @@ struct MG {
   }
 
   void apply_direct(MGLevel<T>& m, T* cor, const T* def) {
-    const int64_t n = m.A.rows;
+    const int64_t n = m.A->rows;
     std::vector<double> b(n);
     for (int64_t i = 0; i < n; ++i) b[i] = double(def[i]);
     for (auto i : *m.filt) b[i] = 0.0;
@@ -385,19 +486,21 @@ struct MG {
   // Richardson(Jacobi) smoother apply(cor, def): richardson.hpp:160-226 with
   // min_iter = max_iter = nu (no defect norms except the initial one, iterative.hpp:744-766)
   int smooth(MGLevel<T>& m, T* cor, const T* def) {
-    const int64_t n = m.A.rows;
+    const int64_t n = m.A->rows;
     T* sd = m.s_def.data();
     T* t = m.s_cor.data();
-    std::copy(def, def + n, sd);
-    std::fill(cor, cor + n, T(0));
+    copy_vec(sd, def, n);
+    fill_vec(cor, T(0), n);
     const T d0 = norm2(sd, n);
     if (!std::isfinite(d0)) return 3;
     if (d0 <= eps<T>() * eps<T>()) return 2;
     for (int it = 0; it < cfg.nu; ++it) {
-      for (int64_t i = 0; i < n; ++i) t[i] = m.inv_diag[i] * sd[i];  // component_product
+      const T* id = m.inv_diag.data();
+#pragma omp parallel for schedule(static) if (n >= kParMin)
+      for (int64_t i = 0; i < n; ++i) t[i] = id[i] * sd[i];  // component_product
       filter_zero(t, *m.filt);
       axpy(cor, t, cor, T(cfg.omega_rich), n);
-      csr_apply(sd, T(-1), cor, T(1), def, m.A);
+      csr_apply(sd, T(-1), cor, T(1), def, *m.A);
       filter_zero(sd, *m.filt);
     }
     return 5;
@@ -405,7 +508,7 @@ struct MG {
 
   // unpreconditioned PCG coarse solver with default settings (pcg.hpp, iterative.hpp:216-235)
   void coarse_pcg(MGLevel<T>& m, T* x, const T* b) {
-    const int64_t n = m.A.rows;
+    const int64_t n = m.A->rows;
     std::vector<T> r(b, b + n), p(n), q(n);
     std::fill(x, x + n, T(0));
     const T tol = std::sqrt(eps<T>());
@@ -415,7 +518,7 @@ struct MG {
     filter_zero(p.data(), *m.filt);
     T gamma = dot(r.data(), p.data(), n);
     for (int it = 1; it <= 100; ++it) {
-      csr_apply(q.data(), T(1), p.data(), T(0), q.data(), m.A);
+      csr_apply(q.data(), T(1), p.data(), T(0), q.data(), *m.A);
       filter_zero(q.data(), *m.filt);
       T alpha = gamma / dot(q.data(), p.data(), n);
       axpy(x, p.data(), x, alpha, n);
@@ -442,10 +545,10 @@ struct MG {
       MGLevel<T>& c = L[i + 1];
       if (cur_smooth || i > cur) {
         smooth(f, f.sol.data(), f.rhs.data());
-        csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+        csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), *f.A);
       }
       filter_zero(f.def.data(), *f.filt);
-      csr_apply(c.rhs.data(), T(1), f.def.data(), T(0), c.rhs.data(), f.R);
+      csr_apply(c.rhs.data(), T(1), f.def.data(), T(0), c.rhs.data(), *f.R);
       filter_zero(c.rhs.data(), *c.filt);
     }
   }
@@ -470,12 +573,12 @@ struct MG {
     for (int i = nl - 2; i >= cur; --i) {
       MGLevel<T>& f = L[i];
       MGLevel<T>& c = L[i + 1];
-      const int64_t n = f.A.rows;
-      csr_apply(f.cor.data(), T(1), c.sol.data(), T(0), f.cor.data(), f.P);
+      const int64_t n = f.A->rows;
+      csr_apply(f.cor.data(), T(1), c.sol.data(), T(0), f.cor.data(), *f.P);
       filter_zero(f.cor.data(), *f.filt);
       T omega = T(1);
       if (cfg.cgc != 0) {
-        csr_apply(f.tmp.data(), T(1), f.cor.data(), T(0), f.tmp.data(), f.A);
+        csr_apply(f.tmp.data(), T(1), f.cor.data(), T(0), f.tmp.data(), *f.A);
         filter_zero(f.tmp.data(), *f.filt);
         if (cfg.cgc == 1) omega = dot(f.def.data(), f.cor.data(), n) / dot(f.tmp.data(), f.cor.data(), n);
         else omega = dot(f.def.data(), f.tmp.data(), n) / dot(f.tmp.data(), f.tmp.data(), n);
@@ -485,7 +588,7 @@ struct MG {
         if (cfg.cgc != 0) {
           axpy(f.def.data(), f.tmp.data(), f.def.data(), -omega, n);
         } else {
-          csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+          csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), *f.A);
           filter_zero(f.def.data(), *f.filt);
         }
         smooth(f, f.cor.data(), f.def.data());
@@ -498,20 +601,20 @@ struct MG {
   // level's (peak = pre = post) smoother to it, correction, defect again
   void smooth_peak(int l) {
     MGLevel<T>& f = L[l];
-    const int64_t n = f.A.rows;
-    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+    const int64_t n = f.A->rows;
+    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), *f.A);
     filter_zero(f.def.data(), *f.filt);
     smooth(f, f.cor.data(), f.def.data());
     filter_zero(f.cor.data(), *f.filt);
     axpy(f.sol.data(), f.cor.data(), f.sol.data(), T(1), n);
-    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), f.A);
+    csr_apply(f.def.data(), T(-1), f.sol.data(), T(1), f.rhs.data(), *f.A);
     filter_zero(f.def.data(), *f.filt);
   }
 
   // MultiGrid::apply (multigrid.hpp:1268-1519): V, F or W cycle
   void vcycle(T* cor_out, const T* def_in) {
-    const int64_t n0 = L[0].A.rows;
-    std::copy(def_in, def_in + n0, L[0].rhs.begin());
+    const int64_t n0 = L[0].A->rows;
+    copy_vec(L[0].rhs.data(), def_in, n0);
     const int last = nl - 1;
     if (cfg.cycle == 1) {
       apply_rest(0, true);
@@ -545,7 +648,7 @@ struct MG {
       apply_coarse();
       apply_prol(0, true);
     }
-    std::copy(L[0].sol.begin(), L[0].sol.end(), cor_out);
+    copy_vec(cor_out, L[0].sol.data(), n0);
   }
 };
 
@@ -587,9 +690,9 @@ struct Precond {
   void apply(double* cor, const double* def, int64_t n) {
     if (mg64) { mg64->vcycle(cor, def); return; }
     d32.resize(n); c32.resize(n);
-    for (int64_t i = 0; i < n; ++i) d32[i] = float(def[i]);
+    convert(d32.data(), def, n);
     mg32->vcycle(c32.data(), d32.data());
-    for (int64_t i = 0; i < n; ++i) cor[i] = double(c32[i]);
+    convert(cor, c32.data(), n);
   }
 };
 
@@ -620,6 +723,7 @@ or_hier* or_hier_create(int dim, int degree, int level, int level_min, const dou
       auto& kc = H->lv[l].k;
       const auto& kf = H->lv[l + 1].k;
       kc.assign(nec, 0.0);
+#pragma omp parallel for schedule(static) if (nec >= kParMin)
       for (int64_t e = 0; e < nec; ++e) {
         int64_t cx = e % Nc, cy = (e / Nc) % Nc, cz = (dim == 3) ? e / (Nc * Nc) : 0;
         double s = 0.0;
@@ -672,7 +776,6 @@ int or_element_matrix(const or_hier* h, int l, double* kref) {
 void or_rhs(const or_hier* h, int kind, double* rhs) {
   const LevelD& L = h->lv[h->level];
   const int d = h->dim, p = h->degree, q1 = p + 1, nloc = h->nloc;
-  std::fill(rhs, rhs + L.n, 0.0);
   GL3 g;
   const double hh = 1.0 / double(L.N);
   const double det = std::pow(0.5 * hh, double(d));
@@ -685,10 +788,13 @@ void or_rhs(const or_hier* h, int kind, double* rhs) {
   auto ebs_xx = [](double x) {
     return (64.0 * x * (1.0 - x) - 8.0) * std::exp(-(2.0 * x - 1.0) * (2.0 * x - 1.0)) / (std::exp(-1.0) - 1.0);
   };
-  std::vector<double> lv(nloc);
+  // element load vectors (independent per element), then each dof sums its elements' entries
+  // in ascending element order: the order of the reference's element-by-element scatter
+  std::vector<double> LV(size_t(L.ne) * nloc, 0.0);
+#pragma omp parallel for schedule(static) if (L.ne >= kParMin)
   for (int64_t e = 0; e < L.ne; ++e) {
     int64_t ec[3] = {e % L.N, (e / L.N) % L.N, (d == 3) ? e / (int64_t(L.N) * L.N) : 0};
-    std::fill(lv.begin(), lv.end(), 0.0);
+    double* lv = LV.data() + size_t(e) * nloc;
     for (int q = 0; q < nq; ++q) {
       int qi[3] = {q % 3, (q / 3) % 3, q / 9};
       double w = det, xq[3], v[3][3], dv[3][3];
@@ -718,7 +824,22 @@ void or_rhs(const or_hier* h, int kind, double* rhs) {
         lv[i] += w * f * phi;
       }
     }
-    for (int i = 0; i < nloc; ++i) rhs[elem_dof(*h, L, e, i)] += lv[i];
+  }
+  const int64_t M1 = L.M + 1;
+#pragma omp parallel for schedule(static) if (L.n >= kParMin)
+  for (int64_t i = 0; i < L.n; ++i) {
+    const int64_t c[3] = {i % M1, (i / M1) % M1, (d == 3) ? i / (M1 * M1) : 0};
+    const Span1 sx = span1(c[0], p, L.N), sy = span1(c[1], p, L.N);
+    const Span1 sz = (d == 3) ? span1(c[2], p, L.N) : Span1{0, 0, 0, 0};
+    double acc = 0.0;
+    for (int64_t ez = sz.e0; ez <= sz.e1; ++ez)
+      for (int64_t ey = sy.e0; ey <= sy.e1; ++ey)
+        for (int64_t ex = sx.e0; ex <= sx.e1; ++ex) {
+          const int64_t e = ex + int64_t(L.N) * (ey + int64_t(L.N) * ez);
+          const int a = int(c[0] - p * ex) + q1 * (int(c[1] - p * ey) + q1 * int(c[2] - p * ez));
+          acc += LV[size_t(e) * nloc + a];
+        }
+    rhs[i] = acc;
   }
   for (auto i : L.filt) rhs[i] = 0.0;
 }
@@ -787,8 +908,9 @@ void or_element_grad(const or_hier* h, const double* u, const double* lam, doubl
   const LevelD& L = h->lv[h->level];
   const int nloc = h->nloc;
   const double sc = h->h_scale(h->level);
-  std::vector<int64_t> loc(nloc);
+#pragma omp parallel for schedule(static) if (L.ne >= kParMin)
   for (int64_t e = 0; e < L.ne; ++e) {
+    int64_t loc[27];
     for (int a = 0; a < nloc; ++a) loc[a] = elem_dof(*h, L, e, a);
     double s = 0.0;
     for (int a = 0; a < nloc; ++a) {

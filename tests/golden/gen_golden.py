@@ -9,6 +9,7 @@ lattice numbering through the DOF coordinates, as compressed .npz files:
     python tests/golden/gen_golden.py --cycles # only the F/W-cycle and adaptive-CGC fixtures
     python tests/golden/gen_golden.py --files  # only the container-file fixtures (feat_files_q1_2d_L3/)
     python tests/golden/gen_golden.py --numbering  # only FEAT's DOF and cell numbering (ref_numbering.npz)
+    python tests/golden/gen_golden.py --full [c2 c3 c4 c5]  # the measured configurations at full size (ref_c*_full_*)
 
 Inputs that are random (coefficient fields, target noise) are drawn here with numpy's
 seeded generator and stored in the fixture next to the outputs.
@@ -107,9 +108,103 @@ def numbering():
     save("ref_numbering", **arrays)
 
 
+def sampled(R, stride):
+    """the reference's solution (and gradient) at every `stride`-th lattice DOF (element), plus
+    norms of the whole vectors: the full-size vectors are too large to keep in the repository"""
+    u = R["u"]
+    out = {"u_stride": stride, "u_sample": u[::stride].copy(), "u_norm2": np.linalg.norm(u),
+           "u_sum": u.sum(), "ndofs": u.size}
+    if "grad" in R:
+        out["grad_sample"] = R["grad"][::stride].copy()
+        out["grad_norm2"] = np.linalg.norm(R["grad"])
+    if "lambda" in R:
+        out["lambda_sample"] = R["lambda"][::stride].copy()
+        out["lambda_norm2"] = np.linalg.norm(R["lambda"])
+    return out
+
+
+def run_full(name, dim, degree, level, rhs, k=None, k_rule=None, stride=97, **kw):
+    R = po.run_ref(dim, degree, level, 1, rhs=rhs, k=k, **kw)
+    info = R["info"]
+    arrays = dict(dim=dim, degree=degree, level=level, level_min=1, rhs_kind=rhs, iters=info["iters"],
+                  status=info["status"], hist=info["hist"], solve_time=info["solve_time"],
+                  setup_time=info["setup_time"], cfg=repr({k_: v for k_, v in kw.items() if k_ != "target"}),
+                  **sampled(R, stride))
+    if k is not None:
+        arrays["k_rule"] = k_rule
+        arrays["k_checksum"] = np.array([k.sum(), (k * k).sum()])
+    save(name, **arrays)
+    shutil.rmtree(R["workdir"], ignore_errors=True)
+    return R
+
+
+def lognormal(n, sigma, seed):
+    return np.exp(sigma * np.random.default_rng(seed).standard_normal(n))
+
+
+def full(which=("c2", "c3", "c4", "c5")):
+    """The measured configurations at their full sizes, solved by the reference itself (minutes of
+    CPU and up to ~30 GB of memory for the 257^3 case). Coefficient fields are regenerated from
+    the stated rule (numpy default_rng(seed).standard_normal), and their checksums are stored."""
+    pcg = dict(solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8)
+    if "c2" in which:
+        full_c2(pcg)
+    if "c3" in which:
+        full_c3(pcg)
+    if "c4" in which:
+        full_c4(pcg)
+    if "c5" in which:
+        full_c5(pcg)
+
+
+def full_c2(pcg):
+    # C2: 3D Q1, 65^3, f = 3 pi^2 prod sin(pi x_i); FP64 MG-PCG V(2,2), and the mixed form FP64
+    # Richardson around ConvertPrecond(FP32 MG) (kernel/solver/convert_precond.hpp:41-120)
+    run_full("ref_c2_full_q1_3d_L6", 3, 1, 6, "sine", **pcg)
+    run_full("ref_c2_full_mixed_richardson_q1_3d_L6", 3, 1, 6, "sine",
+             **dict(pcg, solver="richardson", inner="f32"))
+
+
+def full_c3(pcg):
+    # C3: 2D Q2, 1025^2, k = exp(N(0,1)) per element (seed 3), f = 1; FP64, and FP16-quantised inner matrices
+    k3 = lognormal(512 * 512, 1.0, 3)
+    run_full("ref_c3_full_q2_2d_L9", 2, 2, 9, "one", k=k3, k_rule="exp(default_rng(3).standard_normal(512^2))",
+             **pcg)
+    run_full("ref_c3_full_f16_q2_2d_L9", 2, 2, 9, "one", k=k3, k_rule="exp(default_rng(3).standard_normal(512^2))",
+             **dict(pcg, inner="f16"))
+
+
+def full_c4(pcg):
+    # C4: adjoint on 2D Q1, 513^2, g ~ N(0, 0.25) (sigma 0.5, seed 21), u_target = u(k = 1) + N(0, 1e-2)
+    # noise (sigma 1e-2, seed 22); the reference's FP64 adjoint (dJ/dk_e = -lambda_e^T K_e u_e)
+    lvl = 9
+    u1 = po.run_ref(2, 1, lvl, 1, rhs="one", solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-14)["u"]
+    target = u1 + 1e-2 * np.random.default_rng(22).standard_normal(u1.size)
+    k4 = lognormal(512 * 512, 0.5, 21)
+    R = run_full("ref_c4_full_adjoint_q1_2d_L9", 2, 1, lvl, "one", k=k4,
+                 k_rule="exp(0.5 * default_rng(21).standard_normal(512^2))", target=target, stride=7,
+                 **dict(pcg, tol=1e-14))
+    fn = os.path.join(HERE, "ref_c4_full_adjoint_q1_2d_L9.npz")
+    d = dict(np.load(fn))
+    d["target_rule"] = "u(k=1, tol 1e-14) + 1e-2 * default_rng(22).standard_normal(513^2)"
+    d["target_checksum"] = np.array([target.sum(), (target * target).sum()])
+    d["J"] = 0.5 * float(np.sum((R["u"] - target) ** 2))
+    save("ref_c4_full_adjoint_q1_2d_L9", **d)
+
+
+def full_c5(pcg):
+    # C5: 3D Q1, 257^3, k = exp(N(0,1)) per element (seed 2026: the benchmark's field), f = 1
+    k5 = lognormal(256 ** 3, 1.0, 2026)
+    run_full("ref_c5_full_q1_3d_L8", 3, 1, 8, "one", k=k5, k_rule="exp(default_rng(2026).standard_normal(256^3))",
+             stride=997, **pcg)
+
+
 def main():
     if not po.have_ref():
         sys.exit("oracle/_ref/feat_ref is missing: build it with `make -C oracle ref` first")
+    if "--full" in sys.argv:
+        sel = [a for a in sys.argv[1:] if a in ("c2", "c3", "c4", "c5")]
+        return full(sel or ("c2", "c3", "c4", "c5"))
     if "--cycles" in sys.argv:
         return cycles()
     if "--files" in sys.argv:
