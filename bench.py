@@ -9,6 +9,10 @@ hierarchy resident in HBM (every finest-level operator application streams more 
   e2e    = the same solve through fb_mg_solve_host with pinned host rhs/solution buffers
   fp64   = the plain FP64 GPU MG-PCG (the drop-in, assembled SELL matrices) on the same problem;
            fp64_stencil / fp64_matfree: the FP64 solve on the other storage forms
+  cpu_baseline = the oracle (this project's threaded restatement of the reference solver) solving
+           the same problem at full size on the host cores; its solution gives err_vs_oracle
+--impl reference: the reference's own CPU solver (FEAT3 built from its sources, serial) on the
+  same full-size problem, as many complete timed solves as fit the time budget
 Multi-GPU: replicas only (each rank solves its own copy; no collective on the data path).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--level L] [--impl reference]
@@ -36,19 +40,11 @@ HEAD_KERNEL_NAME = ("k_mf_q1_tiled<float, EpiJacobiK<float,0,0>> finest level (m
                     "inverse diagonal from the cell coefficients, packed FP32 pairs)")
 
 
-def profiled_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from its committed ncu summary (profiles/<kernel>_*.md,
-    line 'dram_bytes_per_launch: N'), or None when no capture has been summarised."""
-    import glob
-    for fn in sorted(glob.glob(os.path.join(ROOT, "profiles", kernel + "_*.md"))):
-        with open(fn) as f:
-            for line in f:
-                if line.strip().startswith("dram_bytes_per_launch:"):
-                    try:
-                        return float(line.split(":", 1)[1].split()[0])
-                    except ValueError:
-                        return None
-    return None
+# DRAM bytes per launch of the dominant kernel (dram__bytes_read.sum + dram__bytes_write.sum) from
+# one ncu capture of that kernel alone; the capture and its scaling to the 257^3 lattice are
+# stated with the figure's command in the design notes. It is a capture figure, not a live
+# measurement of this run.
+HEAD_KERNEL_DRAM_BYTES = 267.8e6
 
 
 def parse():
@@ -59,8 +55,9 @@ def parse():
     ap.add_argument("--level", type=int, default=8, help="refinement level (N = 2^level cells per side)")
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--seed", type=int, default=2026)
-    ap.add_argument("--cpu-level", type=int, default=6, help="size of the bounded CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=240.0,
+                    help="reference arm: seconds of timed full solves (no solve starts that would end past it; at least one)")
     ap.add_argument("--only", default=None,
                     help="profiling aid, e.g. f16, f64-sell, f16-stencil: run just this form's timed solves")
     return ap.parse_args()
@@ -70,8 +67,15 @@ def workload(level):
     n = (2 ** level + 1) ** 3
     return {"workload": f"3D Q1 Poisson, unit cube, {2 ** level}^3 cells ({n:,} DOFs), k=exp(N(0,1)) per element, "
                         f"f=1, Dirichlet 0; PCG + MG V(2,2) Richardson-Jacobi(0.5), levels 1..{level}, direct coarse",
-            "dofs": n, "level": level, "l2": "inputs larger than L2 (126 MB): a finest-level matrix-free FP32 smoothing step streams "
-                  "~340 MB (x, k, rhs, 1/diag, result) at level 8; the assembled FP64 matrix is 5.5 GB"}
+            "dofs": n, "level": level,
+            "l2": "inputs larger than L2 (126 MB): a finest-level matrix-free FP32 smoothing step streams 273 MB "
+                  "(x, k, rhs, result) at level 8; the assembled FP64 matrix is 5.5 GB"}
+
+
+def bench_config(args, world):
+    """the workload both arms report, identically"""
+    return {**workload(args.level), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "seed": args.seed}
 
 
 def coefficient(level, seed):
@@ -116,58 +120,88 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------- CPU reference
-def run_reference_cpu(level, seed, repeat):
-    """The reference's own FP64 MG-PCG (oracle/_ref/feat_ref, FEAT3 built from its sources),
-    serial, same composition, on the level-`level` cube with the same coefficient law."""
+def run_reference_cpu(args):
+    """The reference's own FP64 MG-PCG (oracle/_ref/feat_ref: FEAT3 compiled from its sources, the
+    same composition) on the full-size problem with the same coefficient field, serial (the
+    reference's lafem CPU kernels have no threading). One process: assembly once (untimed), up to
+    min(W, 1) warm-up solves capped at one iteration, then complete solves from a zero initial
+    guess, TimeStamp around Solver::solve only, until K are done or the next would end past the
+    time budget (at least one)."""
     from oracle import pyoracle as po
-    if not po.have_ref():
-        return None
-    k = coefficient(level, seed)
-    times, iters, info = [], [], None
-    for _ in range(repeat):
-        R = po.run_ref(3, 1, level, 1, rhs="one", k=k, solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8)
-        info = R["info"]
-        times.append(float(info["solve_time"]))
-        iters.append(int(info["iters"]))
-    n = (2 ** level + 1) ** 3
-    return {"times": times, "iters": iters, "dofs": n, "setup_s": float(info["setup_time"])}
-
-
-def cpu_baseline_dict(ref, target_dofs, target_iters):
-    t = float(np.median(ref["times"]))
-    rate = ref["dofs"] * ref["iters"][0] / t  # DOF-iterations per second
-    est = target_dofs * target_iters / rate
-    return {"value": est, "unit": "s", "cores": 1, "kind": "reference",
-            "sample": f"reference FEAT3 CPU MG-PCG (oracle/_ref/feat_ref, 1 thread; the reference's lafem CPU "
-                      f"path is serial) on the same problem at {ref['dofs']:,} DOFs: {ref['iters'][0]} iterations in "
-                      f"{t:.3f} s solve time ({rate:.3e} DOF-it/s); value = {target_dofs:,} DOFs x "
-                      f"{target_iters} iterations / that rate",
-            "dof_it_per_s": rate, "sample_solve_s": t, "sample_iters": ref["iters"][0]}
+    k = coefficient(args.level, args.seed)
+    R = po.run_ref(3, 1, args.level, 1, rhs="one", k=k, solver="pcg", nu=2, omega_jac=0.5, coarse="direct",
+                   tol=1e-8, repeat=max(1, args.steps), warmup=min(args.warmup, 1), budget_s=args.ref_budget_s,
+                   outputs=False)
+    info = R["info"]
+    import shutil
+    shutil.rmtree(R["workdir"], ignore_errors=True)
+    times = [float(t) for t in np.atleast_1d(info["solve_times"])]
+    return {"times": times, "iters": int(info["iters"]), "status": int(info["status"]),
+            "setup_s": float(info["setup_time"]), "warmup_solves": int(info.get("warmup_solves", 0)),
+            "final_rel_residual": float(info["def_final"]) / float(info["def_init"])}
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     from oracle import pyoracle as po
     if not po.have_ref():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/feat_ref was not built (reference sources absent at build time)"}))
         return 0
-    lvl = args.cpu_level
-    for _ in range(args.warmup):
-        run_reference_cpu(lvl, args.seed, 1)
-    ref = run_reference_cpu(lvl, args.seed, args.steps)
-    target = (2 ** args.level + 1) ** 3
-    # iterations the same algorithm needs at the bench size: measured by the native arm; the
-    # multigrid iteration count is close to size independent, the sample's own count is used
-    cb = cpu_baseline_dict(ref, target, ref["iters"][0])
-    line = {"metric": METRIC, "impl": "reference", "value": cb["value"], "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(ref["times"])),
+    ref = run_reference_cpu(args)
+    t = float(np.median(ref["times"]))
+    n = (2 ** args.level + 1) ** 3
+    sample = (f"reference FEAT3 CPU MG-PCG (oracle/_ref/feat_ref, 1 thread: the reference's lafem CPU path is "
+              f"serial) on the full problem ({n:,} DOFs): {len(ref['times'])} complete timed solve(s) of "
+              f"{ref['iters']} iterations each (as many as fit in {args.ref_budget_s:.0f} s of timed solving, at "
+              f"least one; {args.steps} requested), median {t:.1f} s; assembly {ref['setup_s']:.1f} s untimed; "
+              f"{ref['warmup_solves']} warm-up solve(s) of one iteration")
+    line = {"metric": METRIC, "impl": "reference", "value": t, "unit": "s", "n_gpus": world,
+            "steps": len(ref["times"]), "steps_requested": args.steps, "warmup": args.warmup,
+            "warmup_run": f"{ref['warmup_solves']} one-iteration solve(s)", "ms_per_step": 1e3 * t,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload(args.level), "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": bench_config(args, world),
+            "cpu_baseline": {"value": t, "unit": "s", "cores": 1, "kind": "reference", "sample": sample,
+                             "solve_times_s": ref["times"], "iters": ref["iters"], "setup_s": ref["setup_s"],
+                             "dof_it_per_s": n * ref["iters"] / t, "host_cores_available": os.cpu_count()},
+            "iters": ref["iters"], "status": ref["status"], "final_rel_residual": ref["final_rel_residual"],
+            "e2e": {"value": t, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
+
+
+def oracle_baseline(args, k, n):
+    """cpu_baseline leg of the native arm: the oracle (the threaded restatement of the reference
+    solver, pinned to the reference's own full-size solve) on the same full-size problem. Returns
+    the cpu_baseline entry and the oracle's FP64 solution, against which the GPU forms' errors are
+    reported."""
+    import time as _t
+    from oracle import pyoracle as po
+    t0 = _t.perf_counter()
+    H = po.Hierarchy(3, 1, args.level, 1, k)
+    b = H.rhs("one")
+    t1 = _t.perf_counter()
+    ref = H.solve(b, solver="pcg", nu=2, omega_jac=0.5, coarse="direct", tol=1e-8)
+    t2 = _t.perf_counter()
+    del H
+    cb = {"value": t2 - t1, "unit": "s", "cores": po.threads(), "kind": "port",
+          "sample": f"the oracle (this project's restatement of the reference's FP64 MG-PCG, independent loops on "
+                    f"{po.threads()} OpenMP threads, reductions sequential) on the full problem ({n:,} DOFs): one "
+                    f"complete solve of {ref['iters']} iterations; assembly {t1 - t0:.1f} s untimed",
+          "iters": ref["iters"], "dof_it_per_s": n * ref["iters"] / (t2 - t1), "host_cores_available": os.cpu_count()}
+    return cb, ref
+
+
+def reference_run_samples(args):
+    """the reference's own 257^3 solution at every 997th DOF (tests/golden/ref_c5_full_q1_3d_L8.npz,
+    made by tests/golden/gen_golden.py from oracle/_ref/feat_ref) when this run solves that problem"""
+    fn = os.path.join(ROOT, "tests", "golden", "ref_c5_full_q1_3d_L8.npz")
+    if args.level != 8 or args.seed != 2026 or not os.path.exists(fn):
+        return None
+    d = np.load(fn)
+    return int(d["u_stride"]), d["u_sample"], int(d["iters"])
 
 
 # ------------------------------------------------------------------------------- ranks
@@ -294,8 +328,11 @@ def native_arm(args):
     clocks = clk.stop()
     umx = rmx["u"]
     err = float(torch.linalg.norm(umx - u64) / torch.linalg.norm(u64))
-    # --- one adjoint gradient solve on the same hierarchy (transposed MG-PCG + element gradient)
-    u_target = (0.9 * umx).contiguous()
+    # --- one adjoint gradient solve on the same hierarchy (transposed MG-PCG + element gradient):
+    # J = 1/2 ||u - u_t||^2 with u_t = u + N(0, (1e-2 max|u|)^2) noise (seed 23)
+    u_host = umx.cpu().numpy()
+    noise = np.random.default_rng(23).standard_normal(n)
+    u_target = torch.tensor(u_host + 1e-2 * np.abs(u_host).max() * noise, device="cuda")
     adj = {}
     for prec in (HEAD_PREC, "f64"):
         mg.configure(precision=prec, format=HEAD_FMT, **common)
@@ -309,7 +346,7 @@ def native_arm(args):
         adj[prec + "_grad"] = grad
     adj_err = float(torch.linalg.norm(adj[HEAD_PREC + "_grad"] - adj["f64_grad"]) / torch.linalg.norm(adj["f64_grad"]))
     adjoint = {"mixed": adj[HEAD_PREC], "fp64": adj["f64"], "grad_rel_diff_mixed_vs_fp64": adj_err,
-               "objective": "J = 1/2 ||u - u_t||^2, u_t = 0.9 u"}
+               "objective": "J = 1/2 ||u - u_t||^2, u_t = u + N(0, (1e-2 max|u|)^2) noise"}
     # --- end to end through the host-buffer entry point
     re2e, te2e, _, _, _ = run_form(HEAD_PREC, max(2, args.steps // 2), 1, host=True, fmt=HEAD_FMT)
 
@@ -355,18 +392,32 @@ def native_arm(args):
     t_fp64s = max_over_ranks(float(np.median(t64s)))
     t_fp64m = max_over_ranks(float(np.median(t64m)))
     t_e2e = max_over_ranks(float(np.median(te2e)))
-    cpu = None
+    cpu, oracle_err, refrun_err = None, None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ref = run_reference_cpu(args.cpu_level, args.seed, 1)
-        if ref is not None:
-            cpu = cpu_baseline_dict(ref, n, it64[-1])
+        cpu, oref = oracle_baseline(args, k, n)
+        uo = oref["u"]
+        forms = {"mixed": umx, "fp64": u64, "fp64_matfree": r64m["u"], "mixed_f16_stencil": rmxs["u"],
+                 "mixed_richardson": rmr["u"]}
+        host = {name: u.cpu().numpy() for name, u in forms.items()}
+        oracle_err = {name: float(np.linalg.norm(u - uo) / np.linalg.norm(uo)) for name, u in host.items()}
+        oracle_err["oracle_iters"] = oref["iters"]
+        samples = reference_run_samples(args)
+        if samples is not None:
+            stride, us, ref_iters = samples
+            refrun_err = {name: float(np.linalg.norm(host[name][::stride] - us) / np.linalg.norm(us))
+                          for name in ("mixed", "fp64", "fp64_matfree")}
+            refrun_err["oracle"] = float(np.linalg.norm(uo[::stride] - us) / np.linalg.norm(us))
+            refrun_err["reference_iters"] = ref_iters
+            refrun_err["what"] = (f"relative error at every {stride}th DOF against the reference's own 257^3 solve "
+                                  "(tests/golden/ref_c5_full_q1_3d_L8.npz, oracle/_ref/feat_ref)")
     if rank == 0:
         line = {
             "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_mixed, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 outer PCG / f32 V-cycle (matrix-free operator)", "data": "synthetic",
-            "config": {**workload(level), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "seed": args.seed},
+            "config": bench_config(args, world),
+            "err_vs_oracle": oracle_err,
+            "err_vs_reference_run": refrun_err,
             "mixed": {"time_s": t_mixed, "iters": itmx[-1], "err_vs_fp64": err,
                       "dof_it_per_s": n * itmx[-1] / t_mixed, "final_rel_residual": rmx["hist"][-1] / rmx["hist"][0],
                       "storage": "matrix-free Q1 operator from per-cell coefficients + matrix-free Q1 transfers"},
@@ -385,7 +436,8 @@ def native_arm(args):
             "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
             "speedup_mixed_vs_fp64_same_storage": t_fp64m / t_mixed,
             "roofline": {"bound": "hbm", "achieved": dom["GBps"], "peak": peak, "unit": "GB/s",
-                         "frac": dom["GBps"] / peak, "traffic": profiled_traffic(HEAD_KERNEL),
+                         "frac": dom["GBps"] / peak, "traffic": HEAD_KERNEL_DRAM_BYTES,
+                         "traffic_source": "ncu capture of the kernel alone (design notes: measurement)",
                          "kernel": HEAD_KERNEL_NAME, "kernels": rf,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650"},
             "adjoint": adjoint,

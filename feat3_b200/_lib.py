@@ -56,6 +56,10 @@ _SIGS = {
     "fb_csr_apply_f32": [vp, flt, vp, flt, vp, vp, vp, vp, u64, u64, u64, i32, vp],
     "fb_ell_apply_f64": [vp, dbl, vp, dbl, vp, vp, vp, vp, vp, u64, u64, vp],
     "fb_ell_apply_f32": [vp, flt, vp, flt, vp, vp, vp, vp, vp, u64, u64, vp],
+    "fb_csr_apply_f64_u64": [vp, dbl, vp, dbl, vp, vp, vp, vp, u64, u64, u64, i32, vp],
+    "fb_csr_apply_f32_u64": [vp, flt, vp, flt, vp, vp, vp, vp, u64, u64, u64, i32, vp],
+    "fb_ell_apply_f64_u64": [vp, dbl, vp, dbl, vp, vp, vp, vp, vp, u64, u64, vp],
+    "fb_ell_apply_f32_u64": [vp, flt, vp, flt, vp, vp, vp, vp, vp, u64, u64, vp],
     "fb_axpy_f64": [vp, dbl, vp, vp, u64, vp],
     "fb_axpy_f32": [vp, flt, vp, vp, u64, vp],
     "fb_dot_f64": [vp, vp, u64, vp, vp],
@@ -76,10 +80,19 @@ _SIGS = {
     "fb_diagonal_csr_f64": [vp, vp, vp, vp, u64, vp],
     "fb_diagonal_csr_f32": [vp, vp, vp, vp, u64, vp],
     "fb_diagonal_ell_f64": [vp, vp, vp, vp, vp, u64, u64, vp],
+    "fb_diagonal_ell_f32": [vp, vp, vp, vp, vp, u64, u64, vp],
+    "fb_diagonal_csr_f64_u64": [vp, vp, vp, vp, u64, vp],
+    "fb_diagonal_csr_f32_u64": [vp, vp, vp, vp, u64, vp],
+    "fb_diagonal_ell_f64_u64": [vp, vp, vp, vp, vp, u64, u64, vp],
+    "fb_diagonal_ell_f32_u64": [vp, vp, vp, vp, vp, u64, u64, vp],
     "fb_unit_filter_rhs_f64": [vp, vp, vp, u64, vp],
     "fb_unit_filter_def_f64": [vp, vp, u64, vp],
     "fb_unit_filter_rhs_f32": [vp, vp, vp, u64, vp],
     "fb_unit_filter_def_f32": [vp, vp, u64, vp],
+    "fb_unit_filter_rhs_f64_u64": [vp, vp, vp, u64, vp],
+    "fb_unit_filter_def_f64_u64": [vp, vp, u64, vp],
+    "fb_unit_filter_rhs_f32_u64": [vp, vp, vp, u64, vp],
+    "fb_unit_filter_def_f32_u64": [vp, vp, u64, vp],
     "fb_convert_f64_to_f32": [vp, vp, u64, vp],
     "fb_convert_f32_to_f64": [vp, vp, u64, vp],
     "fb_set_f64": [vp, dbl, u64, vp],
@@ -103,6 +116,7 @@ _SIGS = {
     "fb_mg_adjoint_grad": [vp, vp, vp, vp, vp, C.POINTER(SolveInfo)],
     "fb_mg_element_grad": [vp, vp, vp, vp],
     "fb_mg_time_spmv": [vp, i32, i32, i32, i32, C.POINTER(dbl)],
+    "fb_mg_test_expire_wait": [vp],
     # container file I/O
     "fb_io_csr_read": [C.c_char_p, i32, C.POINTER(CsrHost)],
     "fb_io_csr_write": [C.c_char_p, i32, C.POINTER(CsrHost), i32],

@@ -53,7 +53,7 @@ def build(force=False, verbose=False, jobs=None):
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
-        cmd = [nvcc()] + ARCH + FLAGS + ["-dc" if False else "-c", src, "-o", obj]
+        cmd = [nvcc()] + ARCH + FLAGS + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -106,13 +106,13 @@ __global__ void k_convert(D* __restrict__ r, const S* __restrict__ x, uint64_t n
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
     r[i] = D(x[i]);
 }
-template<typename T>
-__global__ void k_filter_rhs(T* __restrict__ v, const T* __restrict__ sv, const uint32_t* __restrict__ idx, uint64_t ue) {
+template<typename T, typename IT>
+__global__ void k_filter_rhs(T* __restrict__ v, const T* __restrict__ sv, const IT* __restrict__ idx, uint64_t ue) {
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < ue; i += uint64_t(gridDim.x) * blockDim.x)
     v[idx[i]] = sv[i];
 }
-template<typename T>
-__global__ void k_filter_def(T* __restrict__ v, const uint32_t* __restrict__ idx, uint64_t ue) {
+template<typename T, typename IT>
+__global__ void k_filter_def(T* __restrict__ v, const IT* __restrict__ idx, uint64_t ue) {
   for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < ue; i += uint64_t(gridDim.x) * blockDim.x)
     v[idx[i]] = T(0);
 }
@@ -228,19 +228,35 @@ int fb_scale_f32(float* r, const float* x, float sc, uint64_t n, fb_stream_t s) 
 }
 int fb_unit_filter_rhs_f64(double* v, const double* sv, const uint32_t* idx, uint64_t ue, fb_stream_t s) {
   if (ue && (!v || !sv || !idx)) return FB_ERR_INVALID;
-  return launch_ew(k_filter_rhs<double>, ue, ST(s), v, sv, idx, ue);
+  return launch_ew(k_filter_rhs<double, uint32_t>, ue, ST(s), v, sv, idx, ue);
 }
 int fb_unit_filter_def_f64(double* v, const uint32_t* idx, uint64_t ue, fb_stream_t s) {
   if (ue && (!v || !idx)) return FB_ERR_INVALID;
-  return launch_ew(k_filter_def<double>, ue, ST(s), v, idx, ue);
+  return launch_ew(k_filter_def<double, uint32_t>, ue, ST(s), v, idx, ue);
 }
 int fb_unit_filter_rhs_f32(float* v, const float* sv, const uint32_t* idx, uint64_t ue, fb_stream_t s) {
   if (ue && (!v || !sv || !idx)) return FB_ERR_INVALID;
-  return launch_ew(k_filter_rhs<float>, ue, ST(s), v, sv, idx, ue);
+  return launch_ew(k_filter_rhs<float, uint32_t>, ue, ST(s), v, sv, idx, ue);
 }
 int fb_unit_filter_def_f32(float* v, const uint32_t* idx, uint64_t ue, fb_stream_t s) {
   if (ue && (!v || !idx)) return FB_ERR_INVALID;
-  return launch_ew(k_filter_def<float>, ue, ST(s), v, idx, ue);
+  return launch_ew(k_filter_def<float, uint32_t>, ue, ST(s), v, idx, ue);
+}
+int fb_unit_filter_rhs_f64_u64(double* v, const double* sv, const uint64_t* idx, uint64_t ue, fb_stream_t s) {
+  if (ue && (!v || !sv || !idx)) return FB_ERR_INVALID;
+  return launch_ew(k_filter_rhs<double, uint64_t>, ue, ST(s), v, sv, idx, ue);
+}
+int fb_unit_filter_def_f64_u64(double* v, const uint64_t* idx, uint64_t ue, fb_stream_t s) {
+  if (ue && (!v || !idx)) return FB_ERR_INVALID;
+  return launch_ew(k_filter_def<double, uint64_t>, ue, ST(s), v, idx, ue);
+}
+int fb_unit_filter_rhs_f32_u64(float* v, const float* sv, const uint64_t* idx, uint64_t ue, fb_stream_t s) {
+  if (ue && (!v || !sv || !idx)) return FB_ERR_INVALID;
+  return launch_ew(k_filter_rhs<float, uint64_t>, ue, ST(s), v, sv, idx, ue);
+}
+int fb_unit_filter_def_f32_u64(float* v, const uint64_t* idx, uint64_t ue, fb_stream_t s) {
+  if (ue && (!v || !idx)) return FB_ERR_INVALID;
+  return launch_ew(k_filter_def<float, uint64_t>, ue, ST(s), v, idx, ue);
 }
 int fb_convert_f64_to_f32(float* d, const double* x, uint64_t n, fb_stream_t s) {
   if (n && (!d || !x)) return FB_ERR_INVALID;

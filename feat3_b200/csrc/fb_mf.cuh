@@ -138,6 +138,8 @@ struct MfTile {
   uint32_t dz, dyt;      // grid stride in tiles, as (planes, tiles within a plane) = divmod(gridDim, tpp)
   uint32_t direct_masked;  // the filter is the lattice boundary: every direct-path row is filtered, and
                            // the epilogue of a filtered row does not read the product
+  unsigned* inject;        // test hook (fb_mg_test_expire_wait), or null: while *inject is set, block 0's
+                           // producer clears it and leaves its first stage unfilled (no copy, no arrive)
 };
 
 // tiles of a block in grid-stride order without divisions in the loop
@@ -314,6 +316,13 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
     for (uint32_t t = blockIdx.x; t < G.ntiles; t += gridDim.x, ++it, ti.next(G)) {
       const int s = int(it % NST);
       const uint32_t ph = (it / NST) & 1u;
+      if (G.inject && it == 0 && blockIdx.x == 0) {
+        // test hook: nothing arrives on this stage, so the consumers' bounded wait on it expires
+        // (then the producer's wait on its release, then the drain's); no copy is issued for it
+        unsigned v = 0;
+        if (lane == 0 && *reinterpret_cast<volatile unsigned*>(G.inject)) v = atomicExch(G.inject, 0u);
+        if (__shfl_sync(0xffffffffu, v, 0)) continue;
+      }
       if (it >= NST) {
         const bool okw = lane == 0 ? mbar_wait(&empty[s], ph ^ 1u) : true;
         if (!__shfl_sync(0xffffffffu, okw, 0)) {

@@ -547,6 +547,7 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
   G.nedge_items = (W * W + 15) / 16;
   G.direct_masked = (L.mask_boundary && L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
+  G.inject = m->inject;
   const size_t dyn = size_t(NST) * G.stage_bytes;
   auto fn = k_mf_q1_tiled<T, Epi, NST, MINB, TY, CM1, XT>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
@@ -1332,7 +1333,7 @@ static int body(fb_mg* m) {
     FB_CHECK_LAUNCH();
     FB_TRY(outer_defect(m));
   }
-  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, sizeof(double), cudaMemcpyDeviceToHost, m->stream));
+  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, kHostScalarBytes, cudaMemcpyDeviceToHost, m->stream));
   return FB_OK;
 }
 
@@ -1599,9 +1600,9 @@ int common_init(fb_mg* m) {
   FB_CUDA(cudaMemsetAsync(m->counter, 0, 4 * sizeof(unsigned), m->stream));
   FB_TRY(dalloc(m, &m->dbg_err, 1));
   FB_CUDA(cudaMemsetAsync(m->dbg_err, 0, sizeof(unsigned long long), m->stream));
-  FB_TRY(dalloc(m, &m->kerr, 1));
+  m->kerr = &m->sc->kerr;
+  m->inject = &m->sc->inject;
   FB_TRY(dalloc(m, &m->cred, 64));
-  FB_CUDA(cudaMemsetAsync(m->kerr, 0, sizeof(unsigned), m->stream));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
   FB_CUDA(cudaEventCreate(&m->ev0));
@@ -1638,6 +1639,13 @@ int finish_levels(fb_mg* m) {
   }
   FB_CUDA(cudaStreamSynchronize(m->stream));
   return FB_OK;
+}
+
+// the kernel-wait flag as of the last read-back of the scalars
+static bool host_kerr(const fb_mg* m) {
+  unsigned f = 0;
+  std::memcpy(&f, reinterpret_cast<const char*>(m->host_rr) + offsetof(DevScalars, kerr), sizeof(f));
+  return f != 0;
 }
 
 // a bounded wait inside a staged kernel expired: report it (and clear the flag)
@@ -1687,14 +1695,16 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
       FB_CHECK_LAUNCH();
     }
   }
-  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, sizeof(double), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaMemcpyAsync(m->host_rr, &m->sc->rr, kHostScalarBytes, cudaMemcpyDeviceToHost, s));
   FB_CUDA(cudaStreamSynchronize(s));
   Stop st(m->cfg.tol_rel, m->cfg.max_iter);
   double d = std::sqrt(*m->host_rr);
   int status = st.initial(d);
   int it = 0;
   if (hist) hist[0] = d;
-  while (status == 1) {
+  // a staged kernel whose bounded wait expired has left rows unwritten: the solve stops at the
+  // next read-back and returns FB_ERR_TIMEOUT (check_kernel_waits below)
+  while (status == 1 && !host_kerr(m)) {
     FB_TRY(run_body(m));
     FB_CUDA(cudaStreamSynchronize(s));
     ++it;
@@ -1892,6 +1902,15 @@ int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
   else { k_cvt<double, float><<<ew_grid(n), 256, 0, s>>>(out, (const float*)z, n); FB_CHECK_LAUNCH(); }
   if (m->feat_dof) FB_TRY(perm_from_lattice(m, cor, out, m->feat_dof, n));
   FB_CUDA(cudaStreamSynchronize(s));
+  return FB_OK;
+}
+
+int fb_mg_test_expire_wait(fb_mg* m) {
+  if (!m || !m->inject) return FB_ERR_INVALID;
+  FB_CUDA(cudaSetDevice(m->device));
+  const unsigned one = 1u;
+  FB_CUDA(cudaMemcpyAsync(m->inject, &one, sizeof(one), cudaMemcpyHostToDevice, m->stream));
+  FB_CUDA(cudaStreamSynchronize(m->stream));
   return FB_OK;
 }
 

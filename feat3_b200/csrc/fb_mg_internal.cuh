@@ -1,5 +1,6 @@
 // Internal types of the multigrid driver shared by fb_mg.cu and fb_assembly.cu.
 #pragma once
+#include <cstddef>
 #include "fb_sell.cuh"
 
 #include <vector>
@@ -10,6 +11,8 @@ constexpr int kMaxLevels = 16;
 
 struct DevScalars {
   double rr;            // ||r||^2 of the outer defect
+  unsigned kerr;        // set by a staged kernel whose bounded wait expired; it follows rr so that
+  unsigned kerr_pad;    // one 16-byte copy per outer iteration brings both to the host
   double rz;            // latest r . z
   double gamma;         // previous r . z (PCG)
   double qp;            // q . p
@@ -17,7 +20,12 @@ struct DevScalars {
                         // direction update, or after the last iteration); 0 = none
   double lvl[2 * kMaxLevels];  // [2l] ||rhs_l||^2, [2l+1] ||post-smoothing defect_l||^2
   double tmp[8];
+  unsigned inject;      // test hook of the staged matrix-free kernel (fb_mg_test_expire_wait)
+  unsigned inject_pad;
 };
+// bytes of the scalar block read back per outer iteration: ||r||^2 and the kernel-wait flag
+constexpr size_t kHostScalarBytes = offsetof(DevScalars, kerr_pad) + sizeof(unsigned);
+static_assert(offsetof(DevScalars, kerr) == sizeof(double), "the wait flag follows ||r||^2");
 
 struct DevSell {
   uint32_t rows = 0, cols = 0, nchunks = 0;
@@ -135,7 +143,8 @@ struct fb_mg {
   bool top_s1 = false;
   bool top_dot = false;                  // the V-cycle's last finest-level step also forms r . z
   unsigned long long* dbg_err = nullptr;  // FB_DEBUG=1: device word for kernel self-checks
-  unsigned* kerr = nullptr;               // set by a staged kernel whose bounded wait expired
+  unsigned* kerr = nullptr;               // &sc->kerr: set by a staged kernel whose bounded wait expired
+  unsigned* inject = nullptr;             // &sc->inject (test hook)
   double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)                   // finest-level first smoothing step already formed (fused)
   double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
   double* adj = nullptr;                 // adjoint right-hand side

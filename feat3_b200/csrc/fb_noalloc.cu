@@ -9,7 +9,6 @@
 // allocates or frees device or host memory.
 #include "fb_common.cuh"
 
-#include <cstdio>
 #include <mutex>
 
 namespace fb {
@@ -72,11 +71,7 @@ int fb_dot_f64_noalloc(const double* x, const double* y, uint64_t n, double* res
   // one partial sum per CTA; each CTA covers FB_NOALLOC_DOT_ELEMS_PER_CTA elements
   const uint64_t per_cta = FB_NOALLOC_DOT_ELEMS_PER_CTA;
   const uint64_t grid = n == 0 ? 1 : (n + per_cta - 1) / per_cta;
-  if (n > FB_NOALLOC_DOT_MAX_N || grid > uint64_t(kNoallocMaxPartials)) {
-    std::fprintf(stderr, "fb_dot_f64_noalloc: n = %llu exceeds the fixed scratch limit of %llu elements\n",
-                 (unsigned long long)n, (unsigned long long)FB_NOALLOC_DOT_MAX_N);
-    return FB_ERR_TOO_LARGE;
-  }
+  if (n > FB_NOALLOC_DOT_MAX_N || grid > uint64_t(kNoallocMaxPartials)) return FB_ERR_TOO_LARGE;
   NoallocSymbols s;
   FB_TRY(noalloc_symbols(&s));
   cudaStream_t st = (cudaStream_t)stream;

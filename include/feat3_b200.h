@@ -13,8 +13,9 @@
  *  3. Container file I/O: FEAT3's binary and text formats for matrices and vectors, so a
  *     hierarchy written by a FEAT3 application can be loaded into the solver layer (host code).
  *
- * Conventions: all array pointers of the operator layer are DEVICE pointers; indices are
- * 32-bit unsigned (the reference's 64-bit Index arrays are narrowed once at upload);
+ * Conventions: all array pointers of the operator layer are DEVICE pointers; index arrays are
+ * 32-bit unsigned, or 64-bit unsigned in the *_u64 entry points (FEAT3's default Index), which
+ * read the caller's arrays as they are;
  * sizes are uint64_t; `stream` is a cudaStream_t (NULL = legacy default stream, as the
  * reference uses). Every function returns an int status (FB_OK = 0) and never throws.
  * Functions are asynchronous on `stream` unless their name ends in _sync.
@@ -59,6 +60,17 @@ FB_API int fb_csr_apply_f32(float* r, float a, const float* x, float b, const fl
                      const float* val, const uint32_t* col_ind, const uint32_t* row_ptr,
                      uint64_t rows, uint64_t columns, uint64_t used_elements, int transposed,
                      fb_stream_t stream);
+/* The same with 64-bit index arrays, read as they are (FEAT3's default Index is unsigned long,
+ * kernel/base_header.hpp:95-97). Replaces the unsigned-long overload of Arch::Apply<Mem::CUDA>::csr
+ * (kernel/lafem/arch/apply.hpp:274, apply.cu:25-39,242-269). */
+FB_API int fb_csr_apply_f64_u64(double* r, double a, const double* x, double b, const double* y,
+                     const double* val, const uint64_t* col_ind, const uint64_t* row_ptr,
+                     uint64_t rows, uint64_t columns, uint64_t used_elements, int transposed,
+                     fb_stream_t stream);
+FB_API int fb_csr_apply_f32_u64(float* r, float a, const float* x, float b, const float* y,
+                     const float* val, const uint64_t* col_ind, const uint64_t* row_ptr,
+                     uint64_t rows, uint64_t columns, uint64_t used_elements, int transposed,
+                     fb_stream_t stream);
 
 /* r = b*y + a*A*x, A in FEAT's SELL-C layout (val/col_ind chunk-major with stride C, cs =
  * chunk starts, cl = chunk lengths). Replaces Arch::Apply<Mem::CUDA>::ell
@@ -69,6 +81,14 @@ FB_API int fb_ell_apply_f64(double* r, double a, const double* x, double b, cons
 FB_API int fb_ell_apply_f32(float* r, float a, const float* x, float b, const float* y,
                      const float* val, const uint32_t* col_ind, const uint32_t* cs,
                      const uint32_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
+/* The same with 64-bit index arrays: Arch::Apply<Mem::CUDA>::ell<DT_, unsigned long>
+ * (kernel/lafem/arch/apply.hpp:296). */
+FB_API int fb_ell_apply_f64_u64(double* r, double a, const double* x, double b, const double* y,
+                     const double* val, const uint64_t* col_ind, const uint64_t* cs,
+                     const uint64_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
+FB_API int fb_ell_apply_f32_u64(float* r, float a, const float* x, float b, const float* y,
+                     const float* val, const uint64_t* col_ind, const uint64_t* cs,
+                     const uint64_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
 
 /* r = a*x + y; |a| < eps => r = y. Replaces Arch::Axpy<Mem::CUDA>::dv (axpy.cu:23-55)
  * with the shortcut of DenseVector::axpy (kernel/lafem/dense_vector.hpp:883-905). */
@@ -88,9 +108,12 @@ FB_API int fb_dot_f32_sync(const float* x, const float* y, uint64_t n, double* h
  * forbidden after start-up). Its partial sums live in a fixed device array inside the library
  * (FB_NOALLOC_DOT_MAX_CTAS doubles plus a counter, 32 KiB on every GPU that loads the library,
  * held until exit), so n is limited to FB_NOALLOC_DOT_MAX_N elements; larger n returns
- * FB_ERR_TOO_LARGE. The first call on each device looks up the array's device address; make
- * that first call before any stream capture. All calls share the one array: calls that
- * overlap on the GPU (concurrent streams) race and must be serialised by the caller.
+ * FB_ERR_TOO_LARGE. The first call on each device looks up the array's device address, and
+ * with CUDA's lazy module loading (the default) that lookup may load the library's module,
+ * which allocates device memory for its code and arrays: make one warm-up call per device at
+ * start-up, before allocation is forbidden and before any stream capture. All calls share
+ * the one array: calls that overlap on the GPU (concurrent streams) race and must be
+ * serialised by the caller.
  * *result (device) = x . y, as fb_dot_f64. */
 #define FB_NOALLOC_DOT_MAX_CTAS 4096
 #define FB_NOALLOC_DOT_ELEMS_PER_CTA 16384ull
@@ -121,6 +144,18 @@ FB_API int fb_diagonal_csr_f32(float* diag, const float* val, const uint32_t* co
                         const uint32_t* row_ptr, uint64_t rows, fb_stream_t stream);
 FB_API int fb_diagonal_ell_f64(double* diag, const double* val, const uint32_t* col_ind, const uint32_t* cs,
                         const uint32_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
+FB_API int fb_diagonal_ell_f32(float* diag, const float* val, const uint32_t* col_ind, const uint32_t* cs,
+                        const uint32_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
+/* The same with 64-bit index arrays: Arch::Diagonal<Mem::CUDA>::csr / ::ell<DT_, unsigned long>
+ * (kernel/lafem/arch/diagonal.hpp:69-80). */
+FB_API int fb_diagonal_csr_f64_u64(double* diag, const double* val, const uint64_t* col_ind,
+                        const uint64_t* row_ptr, uint64_t rows, fb_stream_t stream);
+FB_API int fb_diagonal_csr_f32_u64(float* diag, const float* val, const uint64_t* col_ind,
+                        const uint64_t* row_ptr, uint64_t rows, fb_stream_t stream);
+FB_API int fb_diagonal_ell_f64_u64(double* diag, const double* val, const uint64_t* col_ind, const uint64_t* cs,
+                        const uint64_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
+FB_API int fb_diagonal_ell_f32_u64(float* diag, const float* val, const uint64_t* col_ind, const uint64_t* cs,
+                        const uint64_t* cl, uint64_t C, uint64_t rows, fb_stream_t stream);
 
 /* v[idx[i]] = sv[i] / v[idx[i]] = 0. Replaces Arch::UnitFilter<Mem::CUDA>::filter_rhs /
  * filter_def (unit_filter.cu:21-36; used for filter_sol/filter_cor as well,
@@ -129,6 +164,12 @@ FB_API int fb_unit_filter_rhs_f64(double* v, const double* sv_elements, const ui
 FB_API int fb_unit_filter_def_f64(double* v, const uint32_t* sv_indices, uint64_t ue, fb_stream_t stream);
 FB_API int fb_unit_filter_rhs_f32(float* v, const float* sv_elements, const uint32_t* sv_indices, uint64_t ue, fb_stream_t stream);
 FB_API int fb_unit_filter_def_f32(float* v, const uint32_t* sv_indices, uint64_t ue, fb_stream_t stream);
+/* The same with 64-bit index lists: Arch::UnitFilter<Mem::CUDA>::filter_rhs / filter_def
+ * <DT_, unsigned long> (kernel/lafem/arch/unit_filter.hpp:74-81). */
+FB_API int fb_unit_filter_rhs_f64_u64(double* v, const double* sv_elements, const uint64_t* sv_indices, uint64_t ue, fb_stream_t stream);
+FB_API int fb_unit_filter_def_f64_u64(double* v, const uint64_t* sv_indices, uint64_t ue, fb_stream_t stream);
+FB_API int fb_unit_filter_rhs_f32_u64(float* v, const float* sv_elements, const uint64_t* sv_indices, uint64_t ue, fb_stream_t stream);
+FB_API int fb_unit_filter_def_f32_u64(float* v, const uint64_t* sv_indices, uint64_t ue, fb_stream_t stream);
 
 /* precision conversion and fill. Replace MemoryPool<Mem::CUDA>::convert / set_memory
  * (kernel/util/memory_pool.cu:26-41,176-222). */
@@ -303,6 +344,14 @@ FB_API int fb_mg_element_grad(fb_mg* mg, const double* u, const double* lambda, 
  * with q.p, 3 = the same from the FP32-stored direction of the mixed matrix-free form (level 0,
  * precision FB_PREC_F32); precision selects the value storage (FB_PREC_*). */
 FB_API int fb_mg_time_spmv(fb_mg* mg, int level, int which, int precision, int reps, double* ms_per_launch);
+
+/* Test hook, no counterpart in the reference: arms a one-shot flag so that the next launch of
+ * the bulk-staged matrix-free kernel (3D structured levels, FB_FORMAT_MATFREE) leaves one stage
+ * of its first block unfilled. The consumers' bounded wait on that stage expires (after about
+ * one second), the kernel records it and returns, and the solve in progress stops at its next
+ * read-back and returns FB_ERR_TIMEOUT; the handle and the CUDA context stay usable. Nothing but
+ * the tests arms it. */
+FB_API int fb_mg_test_expire_wait(fb_mg* mg);
 
 /* ===================================================================================== */
 /* 3. Container file I/O in FEAT3's formats (host only, no device needed)                */

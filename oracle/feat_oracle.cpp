@@ -15,6 +15,9 @@
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 namespace {
 
@@ -945,6 +948,14 @@ void or_csr_apply(double* r, double a, const double* x, double b, const double* 
       r[row] = (sum * a) + (b * r[row]);
     }
   }
+}
+
+int or_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
 }
 
 }  // extern "C"

@@ -5,8 +5,10 @@
  * __graft_entry__.smoke() and by bench.py's CPU-baseline leg. Nothing in the product
  * (feat3_b200/) may load or call it.
  *
- * It restates, in plain serial C++, the reference algorithms on structured
- * unit-square / unit-cube hierarchies with lexicographic numbering:
+ * It restates, in plain C++, the reference algorithms on structured unit-square /
+ * unit-cube hierarchies with lexicographic numbering (loops whose iterations are
+ * independent run on OpenMP threads and compute what the serial loop computes; the
+ * reductions are sequential, in the reference's order):
  *   - Q1/Q2 Laplace assembly with 3-point Gauss-Legendre per direction
  *       (kernel/assembly/bilinear_operator_assembler.hpp:218-339,
  *        kernel/assembly/common_operators.hpp:36-97, cubature "auto-degree:5")
@@ -91,6 +93,9 @@ void or_csr_apply(double* r, double a, const double* x, double b, const double* 
  * Q1 (degree 1) or Q2 (degree 2) space, cell_lex[c] = lexicographic index of FEAT cell c.
  * Either pointer may be NULL. Returns 0, or -1 for unsupported arguments. */
 int or_feat_numbering(int dim, int degree, int level, uint32_t* dof_lex, uint32_t* cell_lex);
+
+/* threads of the parallel loops (OpenMP), 1 when built without OpenMP */
+int or_threads(void);
 
 #ifdef __cplusplus
 }

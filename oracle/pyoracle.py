@@ -3,8 +3,9 @@
 Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may use
 this module. It wraps
 
-* ``oracle/build/liboracle.so`` -- this project's serial C++ restatement of the reference
-  multigrid path (see ``oracle/feat_oracle.h`` for the reference files it follows), and
+* ``oracle/build/liboracle.so`` -- this project's C++ restatement of the reference multigrid
+  path (see ``oracle/feat_oracle.h`` for the reference files it follows; independent loops on
+  OpenMP threads, reductions sequential), and
 * ``oracle/_ref/feat_ref`` -- the reference's own CPU solver (FEAT3 compiled from its
   sources by ``oracle/Makefile``), driven through files, when that binary exists.
 """
@@ -62,6 +63,8 @@ def lib():
         L.or_csr_apply.argtypes = [vp, d, vp, d, vp, vp, vp, vp, i64, i64, i32]
         L.or_feat_numbering.restype = i32
         L.or_feat_numbering.argtypes = [i32, i32, i32, vp, vp]
+        L.or_threads.restype = i32
+        L.or_threads.argtypes = []
         _lib = L
     return _lib
 
@@ -167,6 +170,11 @@ class Hierarchy:
         return out
 
 
+def threads():
+    """threads the restatement's parallel loops use (1 without OpenMP)"""
+    return int(lib().or_threads())
+
+
 def csr_apply(a, x, b, y, rp, ci, va, rows, cols, transposed=False):
     """r = b*y + a*A*x with the reference's CSR loop (apply_generic.hpp:25-70)."""
     x = np.ascontiguousarray(x, np.float64)
@@ -202,8 +210,8 @@ def _read_info(fn):
             parts = line.split()
             if not parts:
                 continue
-            if parts[0] == "hist":
-                info["hist"] = np.array([float(v) for v in parts[1:]])
+            if parts[0] in ("hist", "solve_times"):
+                info[parts[0]] = np.array([float(v) for v in parts[1:]])
             else:
                 v = parts[1]
                 try:
@@ -215,8 +223,12 @@ def _read_info(fn):
 
 def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", nu=4, omega_jac=0.5,
             omega_rich=1.0, omega_outer=1.0, coarse="direct", tol=1e-8, max_iter=1000, inner="f64",
-            target=None, dump_matrices=False, workdir=None, cycle="v", cgc="fixed", feat_files=False):
-    """Run the reference's own FP64/mixed MG solver; returns info and arrays in lattice order."""
+            target=None, dump_matrices=False, workdir=None, cycle="v", cgc="fixed", feat_files=False,
+            repeat=1, budget_s=0.0, warmup=0, outputs=True):
+    """Run the reference's own FP64/mixed MG solver; returns info and arrays in lattice order.
+    repeat / budget_s / warmup: timed solves from a zero initial guess after `warmup` untimed
+    one-iteration solves, stopping early when the next solve would end past budget_s seconds of
+    timed solving (info["solve_times"]). outputs=False skips reading the solution files back."""
     if not have_ref():
         raise FileNotFoundError(REF_BIN)
     wd = workdir or tempfile.mkdtemp(prefix="feat_ref_")
@@ -226,7 +238,7 @@ def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", n
            "--omega-jac", repr(omega_jac), "--omega-rich", repr(omega_rich),
            "--omega-outer", repr(omega_outer), "--coarse", coarse, "--tol", repr(tol),
            "--maxit", str(max_iter), "--inner", inner, "--out", out, "--quiet", "--cycle", cycle,
-           "--cgc", cgc]
+           "--cgc", cgc, "--repeat", str(repeat), "--budget-s", repr(float(budget_s)), "--warmup", str(warmup)]
     if k is not None:
         kf = os.path.join(wd, "k.bin")
         np.ascontiguousarray(k, np.float64).tofile(kf)
@@ -241,6 +253,8 @@ def run_ref(dim, degree, level, level_min=1, rhs="sine", k=None, solver="pcg", n
         cmd += ["--feat-files"]
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
     info = _read_info(out + ".info")
+    if not outputs:
+        return {"info": info, "workdir": wd, "prefix": out}
     lat = np.fromfile(out + ".lattice", dtype=np.uint64).astype(np.int64)
     n = lat.size
     res = {"info": info, "lattice": lat, "workdir": wd, "prefix": out}

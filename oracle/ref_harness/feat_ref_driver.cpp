@@ -90,6 +90,9 @@ namespace RefDriver
     bool dump_matrices = false;
     bool feat_files = false;       // also write the hierarchy through the reference's own write_out
     bool quiet = false;
+    int repeat = 1;                // timed solves (each from a zero initial guess)
+    double budget_s = 0.0;         // > 0: no further timed solve once the next would end past this
+    int warmup = 0;                // untimed solves of one iteration each before the timed ones
   };
 
   // ---------------------------------------------------------------------------------------
@@ -339,6 +342,7 @@ namespace RefDriver
     const Config& cfg;
     std::deque<std::shared_ptr<Level>> levels; // front = finest
     std::ofstream info;
+    std::vector<double> solve_times;           // every timed solve of the run
 
     explicit Runner(const Config& c) : cfg(c) {}
 
@@ -634,6 +638,10 @@ namespace RefDriver
       info << "status " << status << "\n";
       info << "solve_time " << solve_time << "\n";
       info << "setup_time " << setup_time << "\n";
+      info << "warmup_solves " << cfg.warmup << "\n";
+      info << "solve_times";
+      for(double st : solve_times) info << " " << st;
+      info << "\n";
       info << "def_init " << (hist.empty() ? 0.0 : hist.front()) << "\n";
       info << "def_final " << (hist.empty() ? 0.0 : hist.back()) << "\n";
       info << "hist";
@@ -701,6 +709,35 @@ namespace RefDriver
       return hier;
     }
 
+    // Solver::solve from a zero initial guess, `warmup` times with one iteration (untimed), then
+    // timed (TimeStamp around Solver::solve only, applications/poisson_dirichlet.cpp:198-208)
+    // `repeat` times or until the budget would be exceeded; t = the last timed solve
+    template<typename S_, typename M_, typename F_>
+    void timed_solves(S_& solver, VectorType& vec_sol, const VectorType& vec_rhs, const M_& mat, const F_& filt,
+                      std::vector<double>& hist, int& iters, int& status, double& t)
+    {
+      for(int w(0); w < cfg.warmup; ++w)
+      {
+        solver.set_max_iter(Index(1));
+        vec_sol.format();
+        Solver::solve(solver, vec_sol, vec_rhs, mat, filt);
+      }
+      solver.set_max_iter(Index(cfg.maxit));
+      double total = 0.0;
+      for(int r(0); r < std::max(1, cfg.repeat); ++r)
+      {
+        if(r > 0 && cfg.budget_s > 0.0 && total + t > cfg.budget_s)
+          break;
+        vec_sol.format();
+        TimeStamp at;
+        auto st = Solver::solve(solver, vec_sol, vec_rhs, mat, filt);
+        t = at.elapsed_now();
+        total += t;
+        solve_times.push_back(t);
+        hist = solver.hist; iters = int(solver.get_num_iter()); status = int(st);
+      }
+    }
+
     void solve_f64(VectorType& vec_sol, const VectorType& vec_rhs, std::vector<double>& hist, int& iters, int& status, double& t)
     {
       Level& top = *levels.front();
@@ -713,10 +750,7 @@ namespace RefDriver
         auto solver = std::make_shared<RecPCG<MatrixType, FilterType>>(top.matrix, top.filter, mgv);
         configure(*solver);
         solver->init();
-        TimeStamp at;
-        auto st = Solver::solve(*solver, vec_sol, vec_rhs, top.matrix, top.filter);
-        t = at.elapsed_now();
-        hist = solver->hist; iters = int(solver->get_num_iter()); status = int(st);
+        timed_solves(*solver, vec_sol, vec_rhs, top.matrix, top.filter, hist, iters, status, t);
         solver->done();
       }
       else
@@ -724,10 +758,7 @@ namespace RefDriver
         auto solver = std::make_shared<RecRichardson<MatrixType, FilterType>>(top.matrix, top.filter, cfg.omega_outer, mgv);
         configure(*solver);
         solver->init();
-        TimeStamp at;
-        auto st = Solver::solve(*solver, vec_sol, vec_rhs, top.matrix, top.filter);
-        t = at.elapsed_now();
-        hist = solver->hist; iters = int(solver->get_num_iter()); status = int(st);
+        timed_solves(*solver, vec_sol, vec_rhs, top.matrix, top.filter, hist, iters, status, t);
         solver->done();
       }
       hier->done();
@@ -771,10 +802,7 @@ namespace RefDriver
         auto solver = std::make_shared<RecPCG<MatrixType, FilterType>>(top.matrix, top.filter, conv);
         configure(*solver);
         solver->init();
-        TimeStamp at;
-        auto st = Solver::solve(*solver, vec_sol, vec_rhs, top.matrix, top.filter);
-        t = at.elapsed_now();
-        hist = solver->hist; iters = int(solver->get_num_iter()); status = int(st);
+        timed_solves(*solver, vec_sol, vec_rhs, top.matrix, top.filter, hist, iters, status, t);
         solver->done();
       }
       else
@@ -782,10 +810,7 @@ namespace RefDriver
         auto solver = std::make_shared<RecRichardson<MatrixType, FilterType>>(top.matrix, top.filter, cfg.omega_outer, conv);
         configure(*solver);
         solver->init();
-        TimeStamp at;
-        auto st = Solver::solve(*solver, vec_sol, vec_rhs, top.matrix, top.filter);
-        t = at.elapsed_now();
-        hist = solver->hist; iters = int(solver->get_num_iter()); status = int(st);
+        timed_solves(*solver, vec_sol, vec_rhs, top.matrix, top.filter, hist, iters, status, t);
         solver->done();
       }
       hier->done();
@@ -896,6 +921,9 @@ int main(int argc, char** argv)
     else if(a == "--dump-matrices") cfg.dump_matrices = true;
     else if(a == "--feat-files") cfg.dump_matrices = cfg.feat_files = true;
     else if(a == "--quiet") cfg.quiet = true;
+    else if(a == "--repeat") cfg.repeat = std::atoi(next().c_str());
+    else if(a == "--budget-s") cfg.budget_s = std::atof(next().c_str());
+    else if(a == "--warmup") cfg.warmup = std::atoi(next().c_str());
     else { std::cerr << "unknown option " << a << std::endl; return 2; }
   }
   int rc = 0;
