@@ -37,6 +37,23 @@ def _dev(x, dtype):
     return torch.as_tensor(np.ascontiguousarray(x), dtype=dtype).cuda()
 
 
+def _idx(x, index):
+    """device copy of an index array in FEAT's index type IT_: "u32" (unsigned int) or "u64"
+    (unsigned long, FEAT's default Index); the bits are kept, torch only carries them"""
+    a = np.asarray(x, dtype=np.int64)
+    if index == "u32":
+        if a.size and (a.min() < 0 or a.max() >= 2 ** 32):
+            raise ValueError("32-bit index range exceeded")
+        return _dev(a.astype(np.uint32).view(np.int32), torch.int32)
+    if index == "u64":
+        return _dev(a, torch.int64)
+    raise ValueError(f"index must be 'u32' or 'u64', not {index!r}")
+
+
+def _isfx(index):
+    return "_u64" if index == "u64" else ""
+
+
 class DenseVector:
     """DenseVector<Mem::CUDA, DT> (kernel/lafem/dense_vector.hpp)."""
 
@@ -120,40 +137,45 @@ class DenseVector:
 
 
 class SparseMatrixCSR:
-    """SparseMatrixCSR<Mem::CUDA, DT, u32> with the reference's apply semantics."""
+    """SparseMatrixCSR<Mem::CUDA, DT, IT> with the reference's apply semantics; index = "u32" or
+    "u64" selects IT (unsigned int / unsigned long, the latter FEAT's default Index)."""
 
-    def __init__(self, row_ptr, col_ind, val, columns=None, dtype=torch.float64):
+    def __init__(self, row_ptr, col_ind, val, columns=None, dtype=torch.float64, index="u32"):
         rp = np.asarray(row_ptr)
         self.rows = rp.size - 1
         self.columns = int(columns if columns is not None else self.rows)
         self.nnz = int(rp[-1])
-        if self.nnz >= 2 ** 32 or self.rows >= 2 ** 32:
+        self.index = index
+        if index == "u32" and (self.nnz >= 2 ** 32 or self.rows >= 2 ** 32):
             raise ValueError("32-bit index range exceeded")
-        self.row_ptr = _dev(rp.astype(np.uint32).view(np.int32), torch.int32)
-        self.col_ind = _dev(np.asarray(col_ind).astype(np.uint32).view(np.int32), torch.int32)
+        self.row_ptr = _idx(rp, index)
+        self.col_ind = _idx(col_ind, index)
         self.val = _dev(np.asarray(val, dtype=np.float64), dtype)
 
     @property
     def dtype(self):
         return self.val.dtype
 
+    def _fn(self, op):
+        return f"fb_{op}_{_sfx(self.dtype)}{_isfx(self.index)}"
+
     # r = y + alpha*A*x  (sparse_matrix_csr.hpp:1973-2010);  r = A*x when y is None (:1899-1928)
     def apply(self, r, x, y=None, alpha=1.0, transposed=False):
         b = 0.0 if y is None else 1.0
-        _lib.call(f"fb_csr_apply_{_sfx(self.dtype)}", _p(r.t), alpha, _p(x.t), b, _p(y.t if y is not None else None),
+        _lib.call(self._fn("csr_apply"), _p(r.t), alpha, _p(x.t), b, _p(y.t if y is not None else None),
                   _p(self.val), _p(self.col_ind), _p(self.row_ptr), self.rows, self.columns, self.nnz,
                   1 if transposed else 0, _stream())
         return r
 
     def apply_raw(self, r, a, x, b, y, transposed=False):
         """Arch::Apply::csr signature: r = b*y + a*A*x"""
-        _lib.call(f"fb_csr_apply_{_sfx(self.dtype)}", _p(r.t), a, _p(x.t), b, _p(y.t if y is not None else None),
+        _lib.call(self._fn("csr_apply"), _p(r.t), a, _p(x.t), b, _p(y.t if y is not None else None),
                   _p(self.val), _p(self.col_ind), _p(self.row_ptr), self.rows, self.columns, self.nnz,
                   1 if transposed else 0, _stream())
         return r
 
     def extract_diag(self, d):
-        _lib.call(f"fb_diagonal_csr_{_sfx(self.dtype)}", _p(d.t), _p(self.val), _p(self.col_ind), _p(self.row_ptr),
+        _lib.call(self._fn("diagonal_csr"), _p(d.t), _p(self.val), _p(self.col_ind), _p(self.row_ptr),
                   self.rows, _stream())
         return d
 
@@ -166,16 +188,19 @@ class SparseMatrixCSR:
 
     def write_out(self, mode, filename, symmetric=False):
         from . import fileio
-        m = fileio.CsrFile(self.rows, self.columns, self.row_ptr.cpu().numpy().view(np.uint32).astype(np.uint64),
-                           self.col_ind.cpu().numpy().view(np.uint32).astype(np.uint64),
+        def host(t):
+            a = t.cpu().numpy()
+            return a.view(np.uint32).astype(np.uint64) if a.dtype == np.int32 else a.view(np.uint64)
+        m = fileio.CsrFile(self.rows, self.columns, host(self.row_ptr), host(self.col_ind),
                            self.val.double().cpu().numpy())
         fileio.write_csr(mode, filename, m, symmetric=symmetric)
 
 
 class SparseMatrixELL:
-    """SparseMatrixELL<Mem::CUDA, DT, u32>: FEAT's SELL-C layout (sparse_matrix_ell.hpp:38-63, 865-960)."""
+    """SparseMatrixELL<Mem::CUDA, DT, IT>: FEAT's SELL-C layout (sparse_matrix_ell.hpp:38-63,
+    865-960); index = "u32" or "u64" selects IT."""
 
-    def __init__(self, row_ptr, col_ind, val, columns=None, C=32, dtype=torch.float64):
+    def __init__(self, row_ptr, col_ind, val, columns=None, C=32, dtype=torch.float64, index="u32"):
         rp = np.asarray(row_ptr, dtype=np.int64)
         ci = np.asarray(col_ind, dtype=np.int64)
         va = np.asarray(val, dtype=np.float64)
@@ -197,10 +222,11 @@ class SparseMatrixELL:
             k = np.arange(rl[i])
             ccol[cs[c] + t + k * C] = ci[rp[i]:rp[i + 1]]
             cval[cs[c] + t + k * C] = va[rp[i]:rp[i + 1]]
+        self.index = index
         self.val = _dev(cval, dtype)
-        self.col_ind = _dev(ccol.astype(np.uint32).view(np.int32), torch.int32)
-        self.cs = _dev(cs.astype(np.uint32).view(np.int32), torch.int32)
-        self.cl = _dev(cl.astype(np.uint32).view(np.int32), torch.int32)
+        self.col_ind = _idx(ccol, index)
+        self.cs = _idx(cs, index)
+        self.cl = _idx(cl, index)
 
     @property
     def dtype(self):
@@ -208,35 +234,37 @@ class SparseMatrixELL:
 
     def apply(self, r, x, y=None, alpha=1.0):
         b = 0.0 if y is None else 1.0
-        _lib.call(f"fb_ell_apply_{_sfx(self.dtype)}", _p(r.t), alpha, _p(x.t), b, _p(y.t if y is not None else None),
+        _lib.call(f"fb_ell_apply_{_sfx(self.dtype)}{_isfx(self.index)}", _p(r.t), alpha, _p(x.t), b,
+                  _p(y.t if y is not None else None),
                   _p(self.val), _p(self.col_ind), _p(self.cs), _p(self.cl), self.C, self.rows, _stream())
         return r
 
     def extract_diag(self, d):
-        if self.dtype != torch.float64:
-            raise TypeError("extract_diag is provided for FP64 ELL matrices")
-        _lib.call("fb_diagonal_ell_f64", _p(d.t), _p(self.val), _p(self.col_ind), _p(self.cs), _p(self.cl),
-                  self.C, self.rows, _stream())
+        _lib.call(f"fb_diagonal_ell_{_sfx(self.dtype)}{_isfx(self.index)}", _p(d.t), _p(self.val), _p(self.col_ind),
+                  _p(self.cs), _p(self.cl), self.C, self.rows, _stream())
         return d
 
 
 class UnitFilter:
-    """UnitFilter<Mem::CUDA, DT, u32> (kernel/lafem/unit_filter.hpp)."""
+    """UnitFilter<Mem::CUDA, DT, IT> (kernel/lafem/unit_filter.hpp); index = "u32" or "u64"."""
 
-    def __init__(self, indices, values=None, dtype=torch.float64):
+    def __init__(self, indices, values=None, dtype=torch.float64, index="u32"):
         idx = np.asarray(indices, dtype=np.int64)
         self.ue = idx.size
-        self.idx = _dev(idx.astype(np.uint32).view(np.int32), torch.int32)
+        self.index = index
+        self.idx = _idx(idx, index)
         self.sv = _dev(np.zeros(self.ue) if values is None else np.asarray(values, np.float64), dtype)
 
     def filter_rhs(self, v):
-        _lib.call(f"fb_unit_filter_rhs_{_sfx(v.dtype)}", _p(v.t), _p(self.sv), _p(self.idx), self.ue, _stream())
+        _lib.call(f"fb_unit_filter_rhs_{_sfx(v.dtype)}{_isfx(self.index)}", _p(v.t), _p(self.sv), _p(self.idx),
+                  self.ue, _stream())
         return v
 
     filter_sol = filter_rhs
 
     def filter_def(self, v):
-        _lib.call(f"fb_unit_filter_def_{_sfx(v.dtype)}", _p(v.t), _p(self.idx), self.ue, _stream())
+        _lib.call(f"fb_unit_filter_def_{_sfx(v.dtype)}{_isfx(self.index)}", _p(v.t), _p(self.idx), self.ue,
+                  _stream())
         return v
 
     filter_cor = filter_def

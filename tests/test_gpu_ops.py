@@ -28,14 +28,15 @@ def ref_vectors(n=100):
     return x, y
 
 
+@pytest.mark.parametrize("index", ["u32", "u64"])
 @pytest.mark.parametrize("n", [1, 2, 3, 31, 32, 33, 255, 512])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 @pytest.mark.parametrize("alpha", [0.0, -1.0, 1.234])
-def test_csr_apply_reference_pattern(n, dtype, alpha):
+def test_csr_apply_reference_pattern(n, dtype, alpha, index):
     from feat3_b200.lafem import DenseVector, SparseMatrixCSR
     rp, ci, va = tridiag(n)
     x, y = ref_vectors(n)
-    A = SparseMatrixCSR(rp, ci, va, dtype=dtype)
+    A = SparseMatrixCSR(rp, ci, va, dtype=dtype, index=index)
     r = DenseVector(torch.zeros(n, dtype=dtype, device="cuda"))
     A.apply(r, DenseVector(torch.tensor(x, dtype=dtype).cuda()), DenseVector(torch.tensor(y, dtype=dtype).cuda()), alpha)
     ref = po.csr_apply(alpha, x, 1.0, y, rp, ci, va, n, n)
@@ -43,8 +44,9 @@ def test_csr_apply_reference_pattern(n, dtype, alpha):
     np.testing.assert_allclose(r.numpy(), ref, rtol=tol, atol=tol * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("index", ["u32", "u64"])
 @pytest.mark.parametrize("transposed", [False, True])
-def test_csr_apply_fe_matrix(transposed):
+def test_csr_apply_fe_matrix(transposed, index):
     from feat3_b200.lafem import DenseVector, SparseMatrixCSR
     H = po.Hierarchy(2, 2, 4, 1, k=np.exp(np.random.default_rng(0).standard_normal(16 * 16)))
     rp, ci, va = H.prol(4)  # rectangular: fine x coarse
@@ -52,7 +54,7 @@ def test_csr_apply_fe_matrix(transposed):
     rng = np.random.default_rng(1)
     x = rng.standard_normal(rows if transposed else cols)
     y = rng.standard_normal(cols if transposed else rows)
-    A = SparseMatrixCSR(rp, ci, va, columns=cols)
+    A = SparseMatrixCSR(rp, ci, va, columns=cols, index=index)
     out = DenseVector.zeros(y.size)
     A.apply_raw(out, -0.5, DenseVector(torch.tensor(x).cuda()), 2.0, DenseVector(torch.tensor(y).cuda()), transposed)
     ref = po.csr_apply(-0.5, x, 2.0, y, rp, ci, va, rows, cols, transposed)
@@ -75,25 +77,29 @@ def test_csr_apply_alias_and_zero_beta():
     np.testing.assert_allclose(r2.numpy(), ref2, rtol=1e-14, atol=1e-13 * np.abs(ref2).max())
 
 
+@pytest.mark.parametrize("index", ["u32", "u64"])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
-def test_ell_apply(dtype):
-    from feat3_b200.lafem import DenseVector, SparseMatrixELL
+def test_ell_apply(dtype, index):
+    from feat3_b200.lafem import DenseVector, SparseMatrixCSR, SparseMatrixELL
     H = po.Hierarchy(3, 1, 3, 1)
     rp, ci, va = H.csr()
     n = rp.size - 1
     rng = np.random.default_rng(2)
     x, y = rng.standard_normal(n), rng.standard_normal(n)
-    A = SparseMatrixELL(rp, ci, va, dtype=dtype)
+    A = SparseMatrixELL(rp, ci, va, dtype=dtype, index=index)
     r = DenseVector(torch.zeros(n, dtype=dtype, device="cuda"))
     A.apply(r, DenseVector(torch.tensor(x, dtype=dtype).cuda()), DenseVector(torch.tensor(y, dtype=dtype).cuda()), -1.0)
     ref = po.csr_apply(-1.0, x, 1.0, y, rp, ci, va, n, n)
     tol = 1e-13 if dtype == torch.float64 else 1e-5
     np.testing.assert_allclose(r.numpy(), ref, rtol=tol, atol=tol)
-    d = DenseVector.zeros(n)
-    if dtype == torch.float64:
-        A.extract_diag(d)
-        diag = np.array([va[rp[i]:rp[i + 1]][ci[rp[i]:rp[i + 1]] == i][0] for i in range(n)])
-        np.testing.assert_array_equal(d.numpy(), diag)
+    d = DenseVector.zeros(n, dtype)
+    A.extract_diag(d)
+    diag = np.array([va[rp[i]:rp[i + 1]][ci[rp[i]:rp[i + 1]] == i][0] for i in range(n)])
+    np.testing.assert_array_equal(d.numpy(), diag.astype(d.numpy().dtype))
+    # the CSR diagonal of the same matrix (Diagonal<Mem::CUDA>::csr)
+    dc = DenseVector.zeros(n, dtype)
+    SparseMatrixCSR(rp, ci, va, dtype=dtype, index=index).extract_diag(dc)
+    np.testing.assert_array_equal(dc.numpy(), diag.astype(dc.numpy().dtype))
 
 
 @pytest.mark.parametrize("n", [0, 1, 1000, 1 << 20])
@@ -119,12 +125,13 @@ def test_blas1(n):
     assert X.dot(Y) == X.dot(Y)
 
 
-def test_unit_filter():
+@pytest.mark.parametrize("index", ["u32", "u64"])
+def test_unit_filter(index):
     from feat3_b200.lafem import DenseVector, UnitFilter
     v = np.arange(50, dtype=np.float64)
     idx = np.array([0, 7, 49, 13])
     sv = np.array([-1.0, -2.0, -3.0, -4.0])
-    f = UnitFilter(idx, sv)
+    f = UnitFilter(idx, sv, index=index)
     V = DenseVector(torch.tensor(v).cuda())
     f.filter_rhs(V)
     ref = v.copy()
