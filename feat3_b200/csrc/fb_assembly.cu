@@ -391,6 +391,9 @@ static void build_kref(int dim, int p, std::vector<double>& K, int& nloc) {
   }
 }
 
+// levels of at least this many rows build their assembled copies on first use
+constexpr uint32_t kLazyRows = 1u << 20;
+
 static double elem_scale(int dim, int level) {
   const double h = 1.0 / double(1u << level);
   return std::pow(0.5 * h, double(dim - 2));
@@ -450,11 +453,44 @@ static int build_kron(fb_mg* m, DevCsr& D, int dim, uint32_t rows1, uint32_t col
   return FB_OK;
 }
 
-static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
+// the level's structure without its values: SELL / stencil shapes, the true nonzero count, the
+// stencil offsets and the Dirichlet mask (the lattice boundary)
+static int build_level_meta(fb_mg* m, Level& L, const Geom& g) {
   const uint64_t n = L.n;
   DevSell& S = L.A;
   S.rows = S.cols = uint32_t(n);
   S.nchunks = uint32_t((n + 31) / 32);
+  // true nonzeros: sum of row lengths (closed form per direction)
+  uint64_t nnz1 = 0;
+  for (uint32_t X = 0; X <= g.M; ++X) {
+    uint32_t lo, hi;
+    col_range(X, g, lo, hi);
+    nnz1 += hi - lo + 1;
+  }
+  S.nnz = nnz1 * nnz1 * (g.dim == 3 ? nnz1 : 1);
+  if (g.p == 1) {
+    DevStencil& St = L.St;
+    St.S = g.dim == 3 ? 27 : 9;
+    St.nchunks = S.nchunks;
+    int j = 0;
+    const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
+    for (int dz = z0; dz <= z1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx)
+          St.off[j++] = int32_t((int64_t(dz) * g.M1 + dy) * g.M1 + dx);
+  }
+  FB_TRY(dalloc(m, &L.mask, (n + 31) / 32));
+  k_mask<<<grid_for((n + 31) / 32, 256), 256, 0, m->stream>>>(g, n, L.mask);
+  FB_CHECK_LAUNCH();
+  L.mask_boundary = true;
+  return FB_OK;
+}
+
+// the level's assembled values: SELL (row lengths, chunk starts, columns, FP64 values) and, for Q1,
+// the implicit-column stencil copy (all rows padded to the full 3^dim stencil; absent neighbours = 0)
+static int build_level_values(fb_mg* m, Level& L, const Geom& g, double sc) {
+  const uint64_t n = L.n;
+  DevSell& S = L.A;
   FB_TRY(dalloc(m, &S.rl, n));
   FB_TRY(dalloc(m, &S.cl, S.nchunks));
   FB_TRY(dalloc(m, &S.cs, S.nchunks + 1));
@@ -478,36 +514,33 @@ static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
   k_fill_sell<<<grid_for(uint64_t(S.nchunks) * 32, 128), 128, 0, m->stream>>>(g, n, S.nchunks, S.cs, S.cl, L.k, m->kref,
                                                                              sc, S.col, S.v64);
   FB_CHECK_LAUNCH();
-  // true nonzeros: sum of row lengths (closed form per direction)
-  uint64_t nnz1 = 0;
-  for (uint32_t X = 0; X <= g.M; ++X) {
-    uint32_t lo, hi;
-    col_range(X, g, lo, hi);
-    nnz1 += hi - lo + 1;
-  }
-  S.nnz = nnz1 * nnz1 * (g.dim == 3 ? nnz1 : 1);
   if (g.p == 1) {
-    // implicit-column copy (all rows padded to the full 3^dim stencil; absent neighbours = 0)
     DevStencil& St = L.St;
-    St.S = g.dim == 3 ? 27 : 9;
-    St.nchunks = S.nchunks;
-    int j = 0;
-    const int z0 = g.dim == 3 ? -1 : 0, z1 = g.dim == 3 ? 1 : 0;
-    for (int dz = z0; dz <= z1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx)
-          St.off[j++] = int32_t((int64_t(dz) * g.M1 + dy) * g.M1 + dx);
     const uint64_t ns = uint64_t(St.nchunks) * St.S * 32;
     FB_TRY(dalloc(m, &St.v64, ns));
     FB_CUDA(cudaMemsetAsync(St.v64, 0, sizeof(double) * ns, m->stream));
     k_fill_stencil<<<grid_for(n, 128), 128, 0, m->stream>>>(g, n, L.k, m->kref, sc, St.v64);
     FB_CHECK_LAUNCH();
   }
-  FB_TRY(dalloc(m, &L.mask, (n + 31) / 32));
-  k_mask<<<grid_for((n + 31) / 32, 256), 256, 0, m->stream>>>(g, n, L.mask);
-  FB_CHECK_LAUNCH();
-  L.mask_boundary = true;
   return FB_OK;
+}
+
+static int build_level(fb_mg* m, Level& L, const Geom& g, double sc) {
+  FB_TRY(build_level_meta(m, L, g));
+  return build_level_values(m, L, g, sc);
+}
+
+// diagonal of the level matrix from the row gather that fills the SELL (bit-identical to its
+// stored diagonal entry), without the assembled matrix
+__global__ void k_diag_rows(Geom g, uint64_t n, const double* __restrict__ k, const double* __restrict__ kref,
+                            double sc, double* diag) {
+  const uint64_t row = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  if (row >= n) return;
+  double d = 0.0;
+  row_entries(row, g, k, kref, sc, [&](uint32_t, uint32_t c, double v) {
+    if (c == row) d = v;
+  });
+  diag[row] = d;
 }
 
 static Geom geom_of(const fb_mg* m, int lvl) {
@@ -517,6 +550,36 @@ static Geom geom_of(const fb_mg* m, int lvl) {
   g.M = uint32_t(m->degree) << lvl;
   g.M1 = g.M + 1;
   return g;
+}
+
+// CSR prolongation and restriction between level i and the next coarser one (tensor products
+// of the 1D interpolation, grid_transfer.hpp:304-321 on nested spaces)
+static int build_transfer(fb_mg* m, int i) {
+  const int lvl = m->L[i].lvl_num;
+  const Geom gf = geom_of(m, lvl), gc = geom_of(m, lvl - 1);
+  std::vector<uint32_t> rp, ci, trp, tci;
+  std::vector<double> va, tva;
+  prol1d(m->degree, gf.M, rp, ci, va);
+  transpose1d(gf.M1, gc.M1, rp, ci, va, trp, tci, tva);
+  FB_TRY(build_kron(m, m->L[i].P, m->dim, gf.M1, gc.M1, rp, ci, va));
+  return build_kron(m, m->L[i].R, m->dim, gc.M1, gf.M1, trp, tci, tva);
+}
+
+int ensure_assembled(fb_mg* m, bool matrices, bool transfers) {
+  if (!m->structured) return FB_OK;
+  for (int i = 0; i < (int)m->L.size(); ++i) {
+    Level& L = m->L[i];
+    if (matrices && L.lazy_matrix) {
+      FB_TRY(build_level_values(m, L, geom_of(m, L.lvl_num), elem_scale(m->dim, L.lvl_num)));
+      L.lazy_matrix = false;
+    }
+    if (transfers && L.lazy_transfer) {
+      FB_TRY(build_transfer(m, i));
+      L.lazy_transfer = false;
+    }
+  }
+  FB_CUDA(cudaStreamSynchronize(m->stream));
+  return FB_OK;
 }
 
 }  // namespace fb
@@ -601,7 +664,18 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
     if (st != FB_OK) break;
     for (int i = 0; i < nl && st == FB_OK; ++i) {
       const int lvl = d->level - i;
-      st = build_level(m, m->L[i], geom_of(m, lvl), elem_scale(m->dim, lvl));
+      Level& L = m->L[i];
+      L.lvl_num = lvl;
+      // large 3D Q1 levels: structure now, assembled values on first use (ensure_assembled)
+      L.lazy_matrix = m->dim == 3 && m->degree == 1 && m->mf_ok && L.n >= kLazyRows;
+      st = L.lazy_matrix ? build_level_meta(m, L, geom_of(m, lvl)) : build_level(m, L, geom_of(m, lvl), elem_scale(m->dim, lvl));
+      // the level's diagonal from the row gather (the SELL's diagonal entries, bit for bit)
+      if (st == FB_OK) st = dalloc(m, &L.diag, L.n);
+      if (st == FB_OK) {
+        k_diag_rows<<<grid_for(L.n, 128), 128, 0, m->stream>>>(geom_of(m, lvl), L.n, L.k, m->kref,
+                                                              elem_scale(m->dim, lvl), L.diag);
+        if (cudaGetLastError() != cudaSuccess) st = FB_ERR_CUDA;
+      }
     }
     if (st != FB_OK) break;
     // matrix-free operator data of the Q1 levels
@@ -622,22 +696,21 @@ int fb_mg_create_structured(fb_mg** out, const fb_structured_desc* d) {
       }
     }
     if (st != FB_OK) break;
-    // transfers
+    // transfers (the CSR forms of the large Q1 levels, which only the SELL format uses, on first use)
     for (int i = 0; i + 1 < nl && st == FB_OK; ++i) {
       const int lvl = d->level - i;
       const Geom gf = geom_of(m, lvl), gc = geom_of(m, lvl - 1);
-      std::vector<uint32_t> rp, ci, trp, tci;
-      std::vector<double> va, tva;
-      prol1d(m->degree, gf.M, rp, ci, va);
-      transpose1d(gf.M1, gc.M1, rp, ci, va, trp, tci, tva);
       if (m->degree == 1) {
         Level& Lf = m->L[i];
         Lf.q1_transfer = true;
         Lf.tr.dim = m->dim; Lf.tr.Mf1 = gf.M1; Lf.tr.Mc1 = gc.M1;
         Lf.tr.nf = Lf.n; Lf.tr.nc = m->L[i + 1].n;
       }
-      st = build_kron(m, m->L[i].P, m->dim, gf.M1, gc.M1, rp, ci, va);
-      if (st == FB_OK) st = build_kron(m, m->L[i].R, m->dim, gc.M1, gf.M1, trp, tci, tva);
+      if (m->L[i].lazy_matrix) {
+        m->L[i].lazy_transfer = true;
+        continue;
+      }
+      st = build_transfer(m, i);
     }
     if (st != FB_OK) break;
     // coarse direct solver: coarsest level assembled once more on the host
@@ -698,6 +771,7 @@ int fb_mg_assemble_rhs(fb_mg* m, int kind, double* rhs) {
 int fb_mg_export_csr(fb_mg* m, int l, uint64_t* rp, uint32_t* col, double* val) {
   if (!m || l < 0 || l >= (int)m->L.size() || !rp || !col || !val) return FB_ERR_INVALID;
   FB_CUDA(cudaSetDevice(m->device));
+  FB_TRY(ensure_assembled(m, true, false));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   const DevSell& S = m->L[l].A;
   std::vector<uint32_t> cs(S.nchunks + 1), rl(S.rows), cc(S.nent), perm;

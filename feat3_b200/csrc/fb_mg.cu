@@ -17,6 +17,7 @@
 //     the norm is reduced inside the kernel that produces the defect and read by the next.
 #include "fb_mg_internal.cuh"
 #include "fb_mf.cuh"
+#include "fb_mf_stream.cuh"
 #include "fb_rest_staged.cuh"
 #include "fb_coarse.cuh"
 
@@ -572,6 +573,59 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
   return FB_OK;
 }
 
+// streaming launch (levels of 257^3 and 129^3 points, filter = the lattice boundary): NST stages of
+// TY lines, two CTAs per SM; one contiguous range of slab-lines per CTA
+template<typename T, typename Epi, int TY, int NST, int CM1, typename XT = T>
+static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
+                            double* red_out) {
+  using SE = Staged<Epi>;
+  constexpr int NS = SE::kStreams;
+  constexpr uint32_t M1 = CM1, N = M1 - 1, W = M1 - 2;
+  auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
+  MfStream G{};
+  G.G = std::max<uint32_t>(1, 256 / W);
+  G.nslab = (W + G.G - 1) / G.G;
+  G.units = uint64_t(G.nslab) * W;
+  G.cap_x = r16(uint64_t(TY) * M1 * sizeof(XT)) + 32;
+  G.cap_k = v.k ? r16(uint64_t(TY) * N * sizeof(T)) + 32 : 0;
+  G.cap_s = NS ? r16(uint64_t(TY) * M1 * sizeof(T)) + 32 : 0;
+  G.stage_bytes = ((G.G + 2) * G.cap_x + (G.G + 1) * G.cap_k + NS * G.G * G.cap_s + 127) & ~127u;
+  G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
+  G.nedge_items = (W * W + 15) / 16;
+  G.direct_masked = (L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
+  G.inject = m->inject;
+  const size_t dyn = size_t(NST) * G.stage_bytes;
+  auto fn = k_mf_q1_stream<T, Epi, NST, 2, TY, CM1, XT>;
+  static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
+  if (dyn > attr) {
+    FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+    attr = dyn;
+  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, 288, dyn) != cudaSuccess || bps < 1) {
+    cudaGetLastError();
+    bps = 1;
+  }
+  const uint32_t grid = uint32_t(std::min<uint64_t>(G.units, uint64_t(bps) * kSMs));
+  const T* s0 = NS > 0 ? static_cast<const T*>(SE::stream(epi, 0)) : nullptr;
+  const T* s1 = NS > 1 ? static_cast<const T*>(SE::stream(epi, 1)) : nullptr;
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(288), dyn, v, G, x, epi, s0, s1, m->ws, m->counter, red_out,
+                     m->kerr));
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
+// the streaming kernel takes the FP32 forms and PCG's FP64 q = A p from the FP32 direction on the
+// levels of 257^3 and 129^3 points whose filter is the lattice boundary
+template<typename T, typename Epi, typename XT>
+static bool stream_ok(const fb_mg* m, const Level& L, const Epi& epi) {
+  const bool form = std::is_same<T, float>::value || (std::is_same<T, double>::value && std::is_same<XT, float>::value);
+  const uint32_t* mask = Staged<Epi>::mask(epi);
+  return form && (L.M1 == 257 || L.M1 == 129) && L.mask_boundary && (mask == nullptr || mask == L.mask) &&
+         !(m->cfg.flags & FB_FLAG_NO_STREAM);
+}
+
 // lines per thread and CTAs per SM (measured on the 257^3 solve): FP32 6 lines, 2 CTAs (96
 // registers, no spills; 4 lines at 3 CTAs spilled and ran 2.5 % slower); FP64 2 lines, 2 CTAs
 // (4 % faster than 3 lines), except PCG's q = A p with no streamed inputs: 3 lines (123 us per
@@ -595,6 +649,14 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
                       : (std::is_same<Epi, EpiJacobiK<float, false, false>>::value ||
                          std::is_same<Epi, EpiJacobiK<float, true, false>>::value ||
                          std::is_same<Epi, EpiJacobiK<float, false, true>>::value) ? 7 : TY;
+  if constexpr (std::is_same<T, float>::value || std::is_same<XT, float>::value) {
+    // FP32 ranges: 3 stages of 6 lines; FP64 products (8-byte coefficients): 2 stages
+    constexpr int NSTS = sizeof(T) == 4 ? 3 : 2;
+    if (stream_ok<T, Epi, XT>(m, L, epi)) {
+      if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, NSTS, 257, XT>(m, L, v, x, epi, red_out);
+      return launch_mf_stream<T, Epi, 6, NSTS, 129, XT>(m, L, v, x, epi, red_out);
+    }
+  }
   if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY8, 2, 2, 257, XT>(m, L, v, x, epi, red_out);
   if (L.M1 == 129) return launch_mf_tiled_ty<T, Epi, TY, 2, 2, 129, XT>(m, L, v, x, epi, red_out);
   // the smaller levels have few lines per plane: short tiles spread them over more CTAs
@@ -1633,7 +1695,8 @@ int finish_levels(fb_mg* m) {
       need = std::max<uint64_t>(need, uint64_t((L.tr.Mc1 + 31) / 32) * ((L.tr.Mc1 + 7) / 8) * (L.tr.dim == 3 ? L.tr.Mc1 : 1));
   if (need > 8192) FB_TRY(dalloc(m, &m->ws, need));
   for (auto& L : m->L) {
-    if (!L.diag) FB_TRY(dalloc(m, &L.diag, L.n));
+    if (L.diag) continue;  // structured levels: formed from the row gather at creation
+    FB_TRY(dalloc(m, &L.diag, L.n));
     k_diag_sell<<<grid_for(L.n, 256), 256, 0, m->stream>>>(L.diag, L.A.view(FB_PREC_F64));
     FB_CHECK_LAUNCH();
   }
@@ -1767,11 +1830,11 @@ int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (c->coarse == FB_COARSE_PCG && !m->coarse_csr.rp) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;
   FB_CUDA(cudaSetDevice(m->device));
-  const bool omega_changed = !m->configured || c->omega_jac != m->cfg.omega_jac;
+  // the assembled formats need the level matrices (and SELL the CSR transfers) of the large levels
+  if (c->format != FB_FORMAT_MATFREE) FB_TRY(ensure_assembled(m, true, c->format == FB_FORMAT_SELL));
   m->cfg = *c;
   m->configured = true;
   if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; m->g_body_key = -1; }
-  (void)omega_changed;
   m->prec_built = -1;
   return ensure_vectors(m, c->precision);
 }
@@ -1902,7 +1965,8 @@ int fb_mg_vcycle(fb_mg* m, const double* def, double* cor) {
   else { k_cvt<double, float><<<ew_grid(n), 256, 0, s>>>(out, (const float*)z, n); FB_CHECK_LAUNCH(); }
   if (m->feat_dof) FB_TRY(perm_from_lattice(m, cor, out, m->feat_dof, n));
   FB_CUDA(cudaStreamSynchronize(s));
-  return FB_OK;
+  // a staged kernel whose bounded wait expired left rows unwritten: FB_ERR_TIMEOUT
+  return check_kernel_waits(m);
 }
 
 int fb_mg_test_expire_wait(fb_mg* m) {

@@ -96,7 +96,17 @@ struct Level {
   double kr64[8] = {0};  // (h/2)^(dim-2) K_ref[0][r]
   float kr32[8] = {0};
   float* k32 = nullptr;  // FP32 copy of k
+  // structured 3D Q1 levels of 2^20 rows and more, whose operator runs matrix-free: the assembled
+  // copies (SELL and stencil values) and the CSR transfers are built on first use
+  // (ensure_assembled), so a matrix-free solve never holds them
+  int lvl_num = 0;             // refinement level (structured)
+  bool lazy_matrix = false;    // A / St values not built yet
+  bool lazy_transfer = false;  // P / R (this level <- the next coarser one) not built yet
 };
+
+// builds the deferred assembled matrices (matrices) and CSR transfers (transfers) of a
+// structured hierarchy; a no-op for what exists already
+int ensure_assembled(fb_mg* m, bool matrices, bool transfers);
 
 }  // namespace fb
 

@@ -127,11 +127,12 @@ class MultiGrid:
     # ---------------------------------------------------------------- configuration
     def configure(self, outer="pcg", nu=4, omega_jac=0.5, omega_rich=1.0, omega_outer=1.0, coarse="direct",
                   tol=1e-8, max_iter=1000, precision="f64", graphs=True, format="sell", fuse_coarse=True,
-                  fuse_dot=True, tiled=True, cycle="v", cgc="fixed"):
+                  fuse_dot=True, tiled=True, stream=True, cycle="v", cgc="fixed"):
         """Solver configuration (fb_solver_cfg). cycle: "v", "f" or "w" (Solver::MultiGridCycle);
         cgc: "fixed", "energy" or "defect" (Solver::MultiGridAdaptCGC). fuse_coarse / fuse_dot /
-        tiled switch individual fusions of the matrix-free form off (FB_FLAG_*), for comparisons."""
-        flags = (0 if fuse_coarse else 1) | (0 if fuse_dot else 2) | (0 if tiled else 4)
+        tiled / stream switch individual fusions and kernels of the matrix-free form off
+        (FB_FLAG_*), for comparisons."""
+        flags = (0 if fuse_coarse else 1) | (0 if fuse_dot else 2) | (0 if tiled else 4) | (0 if stream else 8)
         cfg = _lib.SolverCfg(OUTER[outer], nu, omega_jac, omega_rich, omega_outer, COARSE[coarse], tol, max_iter,
                              PRECISION[precision], 1 if graphs else 0, FORMAT[format], flags, CYCLE[cycle], CGC[cgc])
         _lib.check("fb_mg_configure", _lib.load().fb_mg_configure(self.h, C.byref(cfg)))

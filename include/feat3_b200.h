@@ -287,10 +287,12 @@ typedef struct fb_solver_cfg {
 #define FB_CGC_MIN_DEFECT 2
 /* flags: the coarse end of the V-cycle level by level instead of one cluster launch; PCG's
  * r . z as its own reduction instead of inside the last smoothing step; the matrix-free
- * operator without the shared-memory tiled kernel */
+ * operator without the shared-memory tiled kernel; the two finest 3D matrix-free levels with
+ * the line-tiled kernel instead of the streaming one */
 #define FB_FLAG_NO_COARSE_FUSION 1
 #define FB_FLAG_NO_DOT_FUSION 2
 #define FB_FLAG_NO_TILED 4
+#define FB_FLAG_NO_STREAM 8
 FB_API void fb_solver_cfg_default(fb_solver_cfg* cfg);
 FB_API int fb_mg_configure(fb_mg* mg, const fb_solver_cfg* cfg);
 
@@ -315,7 +317,8 @@ FB_API int fb_mg_solve_host(fb_mg* mg, const double* rhs_host, double* sol_host,
 /* The same from a zero initial guess (sol_host is output only, so it is not copied to the device;
  * Solver::solve after vec_sol.format()). */
 FB_API int fb_mg_solve_host_zero(fb_mg* mg, const double* rhs_host, double* sol_host, double* hist, fb_solve_info* info);
-/* one preconditioner application cor = MG(def) on the finest level (device pointers) */
+/* one preconditioner application cor = MG(def) on the finest level (device pointers);
+ * FB_ERR_TIMEOUT when a bounded wait inside a kernel expired (cor is then not valid) */
 FB_API int fb_mg_vcycle(fb_mg* mg, const double* def, double* cor);
 
 /* Load vector of the structured finest level (device output): kind 0 = d*pi^2*prod sin(pi x),

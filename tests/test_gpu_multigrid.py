@@ -265,3 +265,24 @@ def test_c3_full_size_fp16_storage():
         assert mix["status"] == "success" and abs(mix["iters"] - ref["iters"]) <= 1
         assert float(torch.linalg.norm(mix["u"] - u64) / torch.linalg.norm(u64)) <= 1e-8
     mg.close()
+
+
+@pytest.mark.parametrize("lvl", [7, 8])
+def test_stream_kernel_matches_tiled(lvl):
+    """the streaming kernel of the 129^3 and 257^3 matrix-free levels forms each row from the
+    tiled kernel's terms in the tiled kernel's order: one FP32 V-cycle is bit-identical with either
+    kernel; mixed PCG solves (whose q . p sums its CTAs' partials in another grouping) take the
+    same iterations and agree to rounding"""
+    from feat3_b200.solver import MultiGrid
+    k = lognormal_k(3, lvl, 1.0, seed=17)
+    mg = MultiGrid.structured(3, 1, lvl, 1, k)
+    d = mg.assemble_rhs("one")
+    common = dict(nu=2, precision="f32", format="matfree")
+    a = mg.configure(**common).vcycle(d).cpu().numpy()
+    b = mg.configure(stream=False, **common).vcycle(d).cpu().numpy()
+    np.testing.assert_array_equal(a, b)
+    s1 = mg.configure(**common).solve(d)
+    s2 = mg.configure(stream=False, **common).solve(d)
+    assert s1["status"] == s2["status"] == "success" and s1["iters"] == s2["iters"]
+    assert relerr(s1["u"].cpu().numpy(), s2["u"].cpu().numpy()) <= 1e-12
+    mg.close()

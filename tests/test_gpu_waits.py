@@ -43,3 +43,22 @@ def test_expired_wait_returns_timeout_and_handle_recovers(precision, graphs):
         assert after["iters"] == ref["iters"]
     assert relerr(after["u"].cpu().numpy(), ref["u"]) <= tol
     mg.close()
+
+
+def test_expired_wait_in_the_streaming_kernel():
+    """the same through the streaming kernel of the 129^3 level: one FP32 V-cycle, whose first
+    staged launch is the streaming smoother step; the V-cycle returns FB_ERR_TIMEOUT and the next
+    one on the same handle is bit-identical to one before the expiry"""
+    from feat3_b200 import _lib
+    from feat3_b200.solver import MultiGrid
+    k = np.exp(np.random.default_rng(33).standard_normal(128 ** 3))
+    mg = MultiGrid.structured(3, 1, 7, 1, k).configure(nu=2, precision="f32", format="matfree")
+    d = mg.assemble_rhs("one")
+    before = mg.vcycle(d).cpu().numpy()
+    _lib.call("fb_mg_test_expire_wait", mg.h)
+    with pytest.raises(_lib.FeatError) as err:
+        mg.vcycle(d)
+    assert err.value.code == FB_ERR_TIMEOUT
+    after = mg.vcycle(d).cpu().numpy()
+    np.testing.assert_array_equal(after, before)
+    mg.close()
