@@ -616,11 +616,13 @@ static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, con
   return FB_OK;
 }
 
-// the streaming kernel takes the FP32 forms and PCG's FP64 q = A p from the FP32 direction on the
-// levels of 257^3 and 129^3 points whose filter is the lattice boundary
+// the streaming kernel takes the FP32 forms on the levels of 257^3 and 129^3 points whose filter is
+// the lattice boundary (Jacobi step 74.7 against 82.5 us, defect 67.7 against 71.8 us per level-8
+// launch, same box). PCG's FP64 q = A p from the FP32 direction stays on the tiled kernel: its
+// streaming form spills at the 96 registers of two CTAs per SM (111.4 against 96.4 us).
 template<typename T, typename Epi, typename XT>
 static bool stream_ok(const fb_mg* m, const Level& L, const Epi& epi) {
-  const bool form = std::is_same<T, float>::value || (std::is_same<T, double>::value && std::is_same<XT, float>::value);
+  const bool form = std::is_same<T, float>::value && std::is_same<XT, float>::value;
   const uint32_t* mask = Staged<Epi>::mask(epi);
   return form && (L.M1 == 257 || L.M1 == 129) && L.mask_boundary && (mask == nullptr || mask == L.mask) &&
          !(m->cfg.flags & FB_FLAG_NO_STREAM);
@@ -649,12 +651,11 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
                       : (std::is_same<Epi, EpiJacobiK<float, false, false>>::value ||
                          std::is_same<Epi, EpiJacobiK<float, true, false>>::value ||
                          std::is_same<Epi, EpiJacobiK<float, false, true>>::value) ? 7 : TY;
-  if constexpr (std::is_same<T, float>::value || std::is_same<XT, float>::value) {
-    // FP32 ranges: 3 stages of 6 lines; FP64 products (8-byte coefficients): 2 stages
-    constexpr int NSTS = sizeof(T) == 4 ? 3 : 2;
+  if constexpr (std::is_same<T, float>::value && std::is_same<XT, float>::value) {
+    // 3 stages of 6 lines at two CTAs per SM
     if (stream_ok<T, Epi, XT>(m, L, epi)) {
-      if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, NSTS, 257, XT>(m, L, v, x, epi, red_out);
-      return launch_mf_stream<T, Epi, 6, NSTS, 129, XT>(m, L, v, x, epi, red_out);
+      if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, 3, 257, XT>(m, L, v, x, epi, red_out);
+      return launch_mf_stream<T, Epi, 6, 3, 129, XT>(m, L, v, x, epi, red_out);
     }
   }
   if (L.M1 == 257) return launch_mf_tiled_ty<T, Epi, TY8, 2, 2, 257, XT>(m, L, v, x, epi, red_out);
