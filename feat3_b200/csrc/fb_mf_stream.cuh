@@ -8,14 +8,14 @@
 // a run starts with an init stage (x lines Y-1 and Y, cell line Y-1, no rows), and then every
 // stage brings only the lines its TY rows need for the first time (x line Y+1 and cell line Y of
 // each row Y, plus the streamed epilogue inputs). No line is loaded twice within a run, and the
-// stages are small, so NST of them (3 for the FP32 forms) are in flight per CTA at two CTAs per SM.
+// stages are small, so several (NST) are in flight per CTA.
 //
 // The window's line slots are named modulo 3 (x) and modulo 2 (cell lines) by the row's position
 // in its stage; every stage of a run but its last has exactly TY rows (a multiple of 6), so the
 // names repeat from stage to stage and the window never moves between registers.
 //
 // One producer warp issues the stage's bulk copies (cp.async.bulk + mbarrier, each range widened
-// to 16-byte boundaries, which the padded allocations allow); eight consumer warps compute. Rows
+// to 16-byte boundaries, which the padded allocations allow); NCW (8 or 16) consumer warps compute. Rows
 // outside the slabs' interiors (the lattice boundary) are formed first by the consumer warps with
 // direct loads, as in k_mf_q1_tiled. Every mbarrier wait is bounded (about one second); on expiry
 // the kernel records it in `kerr`, stops, waits (bounded) for its own copies and returns.
@@ -64,11 +64,13 @@ struct StreamIter {
   }
 };
 
-template<typename T, typename Epi, int NST, int MINB, int TY, int CM1, typename XT = T>
-__global__ void __launch_bounds__(288, MINB) k_mf_q1_stream(MfView<T, 3> A, MfStream G, const XT* __restrict__ x,
-                                                            Epi epi, const T* st0, const T* st1, double* ws,
-                                                            unsigned* counter, double* red_out, unsigned* kerr) {
+// NCW consumer warps (8 or 16) and one producer warp per CTA
+template<typename T, typename Epi, int NST, int MINB, int TY, int CM1, typename XT = T, int NCW = 8>
+__global__ void __launch_bounds__(32 * (NCW + 1), MINB)
+    k_mf_q1_stream(MfView<T, 3> A, MfStream G, const XT* __restrict__ x, Epi epi, const T* st0, const T* st1,
+                   double* ws, unsigned* counter, double* red_out, unsigned* kerr) {
   static_assert(TY % 6 == 0, "window slots repeat every 6 rows");
+  constexpr int NT = 32 * (NCW + 1);
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr uint32_t M1 = CM1, N = M1 - 1, W = M1 - 2;
@@ -78,12 +80,12 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_stream(MfView<T, 3> A, MfSt
   pdl_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[NST], empty[NST];
-  __shared__ double sh[16];
+  __shared__ double sh[NT / 32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int s = 0; s < NST; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 8);
+      mbar_init(&empty[s], NCW);
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -93,7 +95,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_stream(MfView<T, 3> A, MfSt
   const uint32_t off_k = (Gp + 2) * G.cap_x, off_s = off_k + (Gp + 1) * G.cap_k;
   const uint64_t u0 = G.units * blockIdx.x / gridDim.x, u1 = G.units * (blockIdx.x + 1) / gridDim.x;
   double acc = 0.0;
-  if (warp == 8) {
+  if (warp == NCW) {
     // ---------------- producer: lane q issues range q of the stage
     // (0..G+1: x planes Z0-1..Z0+G; G+2..2G+2: cell planes Z0-1..Z0+G-1; then the streams)
     uint32_t it = 0;
@@ -171,7 +173,7 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_stream(MfView<T, 3> A, MfSt
     {
       const uint32_t cpl = (M1 + 31) / 32;
       const uint32_t nitems = G.nbl_items + G.nedge_items;
-      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
+      for (uint32_t item = blockIdx.x * NCW + warp; item < nitems; item += gridDim.x * NCW) {
         int32_t row = -1;
         uint32_t X = 0, Y = 0, Z = 0;
         if (item < G.nbl_items) {
@@ -367,8 +369,8 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_stream(MfView<T, 3> A, MfSt
   }
   pdl_trigger();
   if (Epi::kReduce) {
-    const double blk = block_sum<288>(acc, sh);
-    reduce_finish<288>(blk, ws, counter, red_out, sh, false);
+    const double blk = block_sum<NT>(acc, sh);
+    reduce_finish<NT>(blk, ws, counter, red_out, sh, false);
   }
 }
 

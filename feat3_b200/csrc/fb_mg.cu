@@ -575,15 +575,16 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 
 // streaming launch (levels of 257^3 and 129^3 points, filter = the lattice boundary): NST stages of
 // TY lines, two CTAs per SM; one contiguous range of slab-lines per CTA
-template<typename T, typename Epi, int TY, int NST, int CM1, typename XT = T>
+template<typename T, typename Epi, int TY, int NST, int CM1, typename XT = T, int NCW = 8, int MINB = 2>
 static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
                             double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr uint32_t M1 = CM1, N = M1 - 1, W = M1 - 2;
+  constexpr int NT = 32 * (NCW + 1);
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
   MfStream G{};
-  G.G = std::max<uint32_t>(1, 256 / W);
+  G.G = std::max<uint32_t>(1, uint32_t(32 * NCW) / W);
   G.nslab = (W + G.G - 1) / G.G;
   G.units = uint64_t(G.nslab) * W;
   G.cap_x = r16(uint64_t(TY) * M1 * sizeof(XT)) + 32;
@@ -595,21 +596,21 @@ static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, con
   G.direct_masked = (L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
   G.inject = m->inject;
   const size_t dyn = size_t(NST) * G.stage_bytes;
-  auto fn = k_mf_q1_stream<T, Epi, NST, 2, TY, CM1, XT>;
+  auto fn = k_mf_q1_stream<T, Epi, NST, MINB, TY, CM1, XT, NCW>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
   if (dyn > attr) {
     FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
     attr = dyn;
   }
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, 288, dyn) != cudaSuccess || bps < 1) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, NT, dyn) != cudaSuccess || bps < 1) {
     cudaGetLastError();
     bps = 1;
   }
   const uint32_t grid = uint32_t(std::min<uint64_t>(G.units, uint64_t(bps) * kSMs));
   const T* s0 = NS > 0 ? static_cast<const T*>(SE::stream(epi, 0)) : nullptr;
   const T* s1 = NS > 1 ? static_cast<const T*>(SE::stream(epi, 1)) : nullptr;
-  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(288), dyn, v, G, x, epi, s0, s1, m->ws, m->counter, red_out,
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(NT), dyn, v, G, x, epi, s0, s1, m->ws, m->counter, red_out,
                      m->kerr));
   m->launches++;
   FB_CHECK_LAUNCH();
@@ -652,9 +653,12 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
                          std::is_same<Epi, EpiJacobiK<float, true, false>>::value ||
                          std::is_same<Epi, EpiJacobiK<float, false, true>>::value) ? 7 : TY;
   if constexpr (std::is_same<T, float>::value && std::is_same<XT, float>::value) {
-    // 3 stages of 6 lines at two CTAs per SM
     if (stream_ok<T, Epi, XT>(m, L, epi)) {
-      if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, 3, 257, XT>(m, L, v, x, epi, red_out);
+      // 257^3: one CTA of 16 consumer warps per SM (slabs of two planes share their x planes), 4
+      // stages of 6 lines (3 with two streamed vectors): 15.21 against 15.40 ms with two CTAs of 8
+      // warps, same box; 129^3: two CTAs of 8 warps, 3 stages (14.5 against 16.2 us per launch)
+      constexpr int NSTW = Staged<Epi>::kStreams > 1 ? 3 : 4;
+      if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, NSTW, 257, XT, 16, 1>(m, L, v, x, epi, red_out);
       return launch_mf_stream<T, Epi, 6, 3, 129, XT>(m, L, v, x, epi, red_out);
     }
   }
