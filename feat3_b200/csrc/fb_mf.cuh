@@ -249,6 +249,78 @@ __device__ __forceinline__ T mf_row_direct(const MfView<T, 3>& A, const XT* __re
   return s;
 }
 
+// ------------------------------------------------------------------ rows outside the tiles
+// The lattice boundary lines in items of 32 consecutive rows ((M1 + 31) / 32 items per line:
+// planes Z = 0 and M1-1 first, then lines Y = 0 and M1-1 of every interior plane), then the two
+// end points of every interior line in items of 16 lines. Item -> this lane's row (-1: none) and
+// its lattice point.
+__device__ __forceinline__ int32_t direct_row(uint32_t item, uint32_t lane, uint32_t M1, uint32_t nbl_items,
+                                              uint32_t& X, uint32_t& Y, uint32_t& Z) {
+  const uint32_t W = M1 - 2, cpl = (M1 + 31) / 32;
+  if (item < nbl_items) {
+    const uint32_t bl = item / cpl;
+    X = (item - bl * cpl) * 32 + lane;
+    if (bl < 2 * M1) {
+      Z = bl < M1 ? 0 : M1 - 1;
+      Y = bl < M1 ? bl : bl - M1;
+    } else {
+      const uint32_t r = bl - 2 * M1;
+      Z = 1 + (r >> 1);
+      Y = (r & 1) ? M1 - 1 : 0;
+    }
+    return X < M1 ? int32_t((Z * M1 + Y) * M1 + X) : -1;
+  }
+  const uint32_t li = (item - nbl_items) * 16 + (lane >> 1);
+  if (li >= W * W) return -1;
+  const uint32_t zq = li / W;
+  Y = 1 + (li - zq * W);
+  Z = 1 + zq;
+  X = (lane & 1) ? M1 - 1 : 0;
+  return int32_t((Z * M1 + Y) * M1 + X);
+}
+
+// One warp's share of the rows outside the tiles (items first, first + stride, ...), epilogue
+// applied; returns the thread's reduction terms in item order. When the epilogue's filter is the
+// lattice boundary (`masked`), every such row is filtered: the product is not formed, and the x
+// and first streamed values of four items (two in FP64) are loaded before any is used, so that a
+// warp's items wait for memory once per four rather than once each. Otherwise A(k) x is formed by
+// gathers.
+template<typename T, typename XT, typename Epi>
+__device__ __forceinline__ double direct_rows(const MfView<T, 3>& A, const XT* __restrict__ x, const Epi& epi,
+                                              const T* st0, bool skp, uint32_t M1, uint32_t nbl_items,
+                                              uint32_t nitems, bool masked, uint32_t first, uint32_t stride,
+                                              uint32_t lane) {
+  using SE = Staged<Epi>;
+  double acc = 0.0;
+  uint32_t X = 0, Y = 0, Z = 0;
+  if (masked) {
+    constexpr int B = sizeof(T) == 4 ? 4 : 2;
+    for (uint32_t i0 = first; i0 < nitems; i0 += B * stride) {
+      int32_t rows[B];
+      T xv[B], sv[B];
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const uint32_t item = i0 + uint32_t(b) * stride;
+        rows[b] = item < nitems ? direct_row(item, lane, M1, nbl_items, X, Y, Z) : -1;
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        xv[b] = rows[b] >= 0 ? T(x[rows[b]]) : T(0);
+        sv[b] = (SE::kStreams > 0 && rows[b] >= 0) ? st0[rows[b]] : T(0);
+      }
+#pragma unroll
+      for (int b = 0; b < B; ++b)
+        if (rows[b] >= 0) acc += SE::apply(epi, skp, uint32_t(rows[b]), T(0), xv[b], &sv[b], true, T(0));
+    }
+    return acc;
+  }
+  for (uint32_t item = first; item < nitems; item += stride) {
+    const int32_t row = direct_row(item, lane, M1, nbl_items, X, Y, Z);
+    if (row >= 0) acc += epi(uint32_t(row), mf_row_direct<T, XT>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z)));
+  }
+  return acc;
+}
+
 // sums of the cell coefficients of cell line c (kw[oz][c][ox]) over the cells that a
 // neighbour offset (dz, dx) in {-1,0,1}^2 selects: -1 -> the lower cell, +1 -> the upper one,
 // 0 -> both; K[dz+1][dx+1]
@@ -378,37 +450,12 @@ __global__ void __launch_bounds__(288, MINB) k_mf_q1_tiled(MfView<T, 3> A, MfTil
     }
     __syncwarp();
   } else {
-    // ---------------- direct path first: boundary lines and the end points of interior lines
-    // (rows no tile holds; done while the producer fills the first stages)
-    {
-      const uint32_t cpl = (M1 + 31) / 32;  // chunks per boundary line
-      const uint32_t nitems = G.nbl_items + G.nedge_items;
-      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
-        int32_t row = -1;
-        uint32_t X = 0, Y = 0, Z = 0;
-        if (item < G.nbl_items) {
-          const uint32_t bl = item / cpl;
-          X = (item - bl * cpl) * 32 + lane;
-          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl < M1 ? bl : bl - M1; }
-          else { const uint32_t r = bl - 2 * M1; Z = 1 + (r >> 1); Y = (r & 1) ? M1 - 1 : 0; }
-          if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
-        } else {
-          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
-          if (li < W * W) {
-            const uint32_t zq = li / W;
-            Y = 1 + (li - zq * W); Z = 1 + zq;
-            X = (lane & 1) ? M1 - 1 : 0;
-            row = int32_t((Z * M1 + Y) * M1 + X);
-          }
-        }
-        if (row >= 0) {
-          const T s = G.direct_masked ? T(0) : mf_row_direct<T, XT>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
-          acc += epi(uint32_t(row), s);
-        }
-      }
-    }
-    // ---------------- consumers: TY rows per thread and tile (sliding window along Y)
+    // ---------------- direct path first: the rows no tile holds, while the producer fills the
+    // first stages
     const bool skp = SE::skip(epi);
+    acc += direct_rows<T, XT, Epi>(A, x, epi, st0, skp, M1, G.nbl_items, G.nbl_items + G.nedge_items,
+                                   G.direct_masked != 0, blockIdx.x * 8 + warp, gridDim.x * 8, lane);
+    // ---------------- consumers: TY rows per thread and tile (sliding window along Y)
     const uint32_t tid = threadIdx.x;
     const uint32_t grp = tid / W, X = 1 + (tid - grp * W);
     const bool active = grp < G.G;

@@ -1,8 +1,8 @@
 // Streaming form of the matrix-free Q1 operator on the two finest structured 3D levels
 // (lattice size a compile-time constant), with the epilogues of k_mf_q1_tiled.
 //
-// The interior planes form slabs of G consecutive planes, one thread group of W = M1 - 2 threads
-// per plane and one thread per interior point X of a line. The slab-lines (slab, interior line Y)
+// The interior planes form slabs of G consecutive planes, one thread group per plane and one thread
+// per interior point X of a line (or per two, CPT = 2). The slab-lines (slab, interior line Y)
 // are numbered u = slab * W + (Y - 1), and each CTA takes one contiguous range of them, walking up
 // the lines of a slab with a sliding 3x3x3 register window that it carries from stage to stage:
 // a run starts with an init stage (x lines Y-1 and Y, cell line Y-1, no rows), and then every
@@ -15,7 +15,7 @@
 // names repeat from stage to stage and the window never moves between registers.
 //
 // One producer warp issues the stage's bulk copies (cp.async.bulk + mbarrier, each range widened
-// to 16-byte boundaries, which the padded allocations allow); NCW (8 or 16) consumer warps compute. Rows
+// to 16-byte boundaries, which the padded allocations allow); NCW (8, 12 or 16) consumer warps compute. Rows
 // outside the slabs' interiors (the lattice boundary) are formed first by the consumer warps with
 // direct loads, as in k_mf_q1_tiled. Every mbarrier wait is bounded (about one second); on expiry
 // the kernel records it in `kerr`, stops, waits (bounded) for its own copies and returns.
@@ -64,12 +64,18 @@ struct StreamIter {
   }
 };
 
-// NCW consumer warps (8 or 16) and one producer warp per CTA
-template<typename T, typename Epi, int NST, int MINB, int TY, int CM1, typename XT = T, int NCW = 8>
-__global__ void __launch_bounds__(32 * (NCW + 1), MINB)
-    k_mf_q1_stream(MfView<T, 3> A, MfStream G, const XT* __restrict__ x, Epi epi, const T* st0, const T* st1,
-                   double* ws, unsigned* counter, double* red_out, unsigned* kerr) {
+// NCW consumer warps (8, 12 or 16) and one producer warp per CTA. CPT = 2: each consumer thread forms
+// two adjacent rows X0 = 1 + 2t and X0 + 1 of a line from one window of 4 columns and 3 cells
+// (packed FP32 form only); the last thread of an odd-width line computes its second row on the
+// lattice boundary from in-slot data and does not store it.
+template<typename T, typename Epi, int NST, int TY, int CM1, typename XT, int NCW, int CPT>
+__device__ __forceinline__ void mf_stream_body(const MfView<T, 3>& A, const MfStream& G, const XT* __restrict__ x,
+                                               const Epi& epi, const T* st0, const T* st1, double* ws,
+                                               unsigned* counter, double* red_out, unsigned* kerr) {
   static_assert(TY % 6 == 0, "window slots repeat every 6 rows");
+  static_assert(CPT == 1 || (CPT == 2 && std::is_same<T, float>::value && std::is_same<XT, float>::value &&
+                             Staged<Epi>::kStreams <= 1),
+                "two rows per thread: packed FP32 form, at most one streamed vector");
   constexpr int NT = 32 * (NCW + 1);
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
@@ -169,41 +175,130 @@ __global__ void __launch_bounds__(32 * (NCW + 1), MINB)
     }
     __syncwarp();
   } else {
-    // ---------------- direct path first: boundary lines and the end points of interior lines
-    {
-      const uint32_t cpl = (M1 + 31) / 32;
-      const uint32_t nitems = G.nbl_items + G.nedge_items;
-      for (uint32_t item = blockIdx.x * NCW + warp; item < nitems; item += gridDim.x * NCW) {
-        int32_t row = -1;
-        uint32_t X = 0, Y = 0, Z = 0;
-        if (item < G.nbl_items) {
-          const uint32_t bl = item / cpl;
-          X = (item - bl * cpl) * 32 + lane;
-          if (bl < 2 * M1) { Z = bl < M1 ? 0 : M1 - 1; Y = bl < M1 ? bl : bl - M1; }
-          else { const uint32_t r = bl - 2 * M1; Z = 1 + (r >> 1); Y = (r & 1) ? M1 - 1 : 0; }
-          if (X < M1) row = int32_t((Z * M1 + Y) * M1 + X);
-        } else {
-          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
-          if (li < W * W) {
-            const uint32_t zq = li / W;
-            Y = 1 + (li - zq * W); Z = 1 + zq;
-            X = (lane & 1) ? M1 - 1 : 0;
-            row = int32_t((Z * M1 + Y) * M1 + X);
-          }
-        }
-        if (row >= 0) {
-          const T s = G.direct_masked ? T(0) : mf_row_direct<T, XT>(A, x, row, int32_t(X), int32_t(Y), int32_t(Z));
-          acc += epi(uint32_t(row), s);
-        }
-      }
-    }
-    // ---------------- consumers
+    // ---------------- direct path first: the rows outside the slabs' interiors
     const bool skp = SE::skip(epi);
+    acc += direct_rows<T, XT, Epi>(A, x, epi, st0, skp, M1, G.nbl_items, G.nbl_items + G.nedge_items,
+                                   G.direct_masked != 0, blockIdx.x * NCW + warp, gridDim.x * NCW, lane);
+    // ---------------- consumers
     const uint32_t tid = threadIdx.x;
-    const uint32_t grp = tid / W, X = 1 + (tid - grp * W);
+    constexpr uint32_t PW = (W + CPT - 1) / CPT;  // threads per line
+    const uint32_t grp = tid / PW, X = 1 + CPT * (tid - grp * PW);
     uint32_t it = 0;
     StreamIter<W, TY> sit(u0, u1);
     StreamStep stp;
+    if constexpr (CPT == 2) {
+      // window of 4 columns X-1..X+2 and 3 cells X-1, X, X+1: xp/xm [slot][column], kp [cell];
+      // Kp / Km [slot][i]: i = 0, 2, 4 the cells, i = 1, 3 the sums of neighbouring cells, so row X
+      // takes Kp[.][0..2] and columns 0..2, row X+1 takes Kp[.][2..4] and columns 1..3
+      float2 xp2[3][4], Kp2[2][5];
+      float xm2[3][4], Km2[2][5];
+      const bool second = X + 1 <= W;  // the second row is an interior row
+      while (sit.next(stp)) {
+        const int s = int(it % NST);
+        const uint32_t ph = (it / NST) & 1u;
+        if (!mbar_wait(&full[s], ph)) {
+          atomicExch(kerr, 3u);
+          break;
+        }
+        const unsigned char* st = smem + size_t(s) * G.stage_bytes;
+        const uint32_t Z0 = 1 + stp.slab * Gp, Z = Z0 + grp;
+        if (grp < Gp && Z <= W) {
+          const uint32_t xl0 = stp.init ? stp.y - 1 : stp.y + 1;
+          const uint32_t kl0 = stp.init ? stp.y - 1 : stp.y;
+          const float* xs[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            const uint64_t lo = (uint64_t(Z - 1 + q) * M1 + xl0) * M1;
+            xs[q] = reinterpret_cast<const float*>(st + (grp + q) * G.cap_x) + (lo & (EX - 1)) + X;
+          }
+          const float* ks[2];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const uint64_t lo = (uint64_t(Z - 1 + q) * N + kl0) * N;
+            ks[q] = reinterpret_cast<const float*>(st + off_k + (grp + q) * G.cap_k) + (lo & (E - 1)) + (X - 1);
+          }
+          // cell sums of one cell line: cells X-1, X, X+1 paired over the cell planes Z-1 / Z
+          auto cells = [&](int slot, int off) {
+            float2 c[3];
+#pragma unroll
+            for (int e = 0; e < 3; ++e) c[e] = A.k ? make_float2(ks[0][off + e], ks[1][off + e]) : make_float2(1.f, 1.f);
+            Kp2[slot][0] = c[0];
+            Kp2[slot][2] = c[1];
+            Kp2[slot][4] = c[2];
+            Kp2[slot][1] = __fadd2_rn(c[0], c[1]);
+            Kp2[slot][3] = __fadd2_rn(c[1], c[2]);
+#pragma unroll
+            for (int i = 0; i < 5; ++i) Km2[slot][i] = Kp2[slot][i].x + Kp2[slot][i].y;
+          };
+          if (stp.init) {
+#pragma unroll
+            for (int l = 0; l < 2; ++l)
+#pragma unroll
+              for (int d = 0; d < 4; ++d) {
+                xp2[l][d] = make_float2(xs[0][l * int(M1) + d - 1], xs[2][l * int(M1) + d - 1]);
+                xm2[l][d] = xs[1][l * int(M1) + d - 1];
+              }
+            cells(0, 0);
+          } else {
+            const uint64_t r0 = (uint64_t(Z) * M1 + stp.y) * M1;
+            const float* ss = reinterpret_cast<const float*>(st + off_s + grp * G.cap_s) + (r0 & (E - 1)) + X;
+            auto rows = [&](auto fast) {
+              constexpr bool FAST = decltype(fast)::value;
+#pragma unroll
+              for (int j = 0; j < TY; ++j) {
+                if (!FAST && uint32_t(j) >= stp.nl) break;
+                const int a = j % 3, b = (j + 1) % 3, c = (j + 2) % 3, ka = j % 2, kb = (j + 1) % 2;
+#pragma unroll
+                for (int d = 0; d < 4; ++d) {
+                  xp2[c][d] = make_float2(xs[0][j * int(M1) + d - 1], xs[2][j * int(M1) + d - 1]);
+                  xm2[c][d] = xs[1][j * int(M1) + d - 1];
+                }
+                cells(kb, j * int(N));
+                // (Kp[ka][2] + Kp[kb][2]) is S5's far-cell sum of row X and its near-cell sum of row X+1
+                const float2 K2 = __fadd2_rn(Kp2[ka][2], Kp2[kb][2]);
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                  // row X + o: columns o..o+2, cells Kp2[.][2o..2o+2]; the terms and order of the
+                  // single-row packed form
+                  const int i0 = 2 * o, i1 = 2 * o + 1, i2 = 2 * o + 2;
+                  const float kc = Km2[ka][i1] + Km2[kb][i1];
+                  const float2 K0 = o == 0 ? __fadd2_rn(Kp2[ka][i0], Kp2[kb][i0]) : K2;
+                  const float2 Kf = o == 0 ? K2 : __fadd2_rn(Kp2[ka][i2], Kp2[kb][i2]);
+                  float2 S5 = __fmul2_rn(K0, xp2[b][o]);
+                  S5 = __ffma2_rn(Kf, xp2[b][o + 2], S5);
+                  float2 S6 = __fmul2_rn(Kp2[ka][i1], xp2[a][o + 1]);
+                  S6 = __ffma2_rn(Kp2[kb][i1], xp2[c][o + 1], S6);
+                  float2 S7 = __fmul2_rn(Kp2[ka][i0], xp2[a][o]);
+                  S7 = __ffma2_rn(Kp2[ka][i2], xp2[a][o + 2], S7);
+                  S7 = __ffma2_rn(Kp2[kb][i0], xp2[c][o], S7);
+                  S7 = __ffma2_rn(Kp2[kb][i2], xp2[c][o + 2], S7);
+                  const float S0 = kc * xm2[b][o + 1];
+                  float S3 = Km2[ka][i0] * xm2[a][o];
+                  S3 += Km2[ka][i2] * xm2[a][o + 2];
+                  S3 += Km2[kb][i0] * xm2[c][o];
+                  S3 += Km2[kb][i2] * xm2[c][o + 2];
+                  float sum = A.kr[0] * S0;
+                  sum += A.kr[3] * S3;
+                  sum += A.kr[5] * (S5.x + S5.y);
+                  sum += A.kr[6] * (S6.x + S6.y);
+                  sum += A.kr[7] * (S7.x + S7.y);
+                  const float xc = xm2[b][o + 1];
+                  const uint32_t row = uint32_t(r0) + uint32_t(j) * M1 + X + o;
+                  T sv[1];
+                  if (NS > 0) sv[0] = ss[j * int(M1) + o];
+                  if (o == 0 || second) acc += SE::apply(epi, FAST ? false : skp, row, sum, xc, sv, false, kc);
+                }
+              }
+            };
+            if (!skp && A.k && stp.nl == uint32_t(TY)) rows(std::true_type{});
+            else rows(std::false_type{});
+          }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        ++it;
+      }
+    } else {
     // window: xp[slot][dx] pairs planes Z-1 / Z+1, xm[slot][dx] is plane Z, kp[slot][ex] pairs cell
     // planes Z-1 / Z (packed FP32 form); xw[plane][slot][dx], kw[cell plane][slot][ex] (scalar form)
     float2 xp[3][3], kp[2][2], Kp[2][3];
@@ -366,12 +461,39 @@ __global__ void __launch_bounds__(32 * (NCW + 1), MINB)
       if (lane == 0) mbar_arrive(&empty[s]);
       ++it;
     }
+    }
   }
   pdl_trigger();
   if (Epi::kReduce) {
     const double blk = block_sum<NT>(acc, sh);
     reduce_finish<NT>(blk, ws, counter, red_out, sh, false);
   }
+}
+
+// 8 consumer warps: two CTAs per SM at up to 96 registers
+template<typename T, typename Epi, int NST, int MINB, int TY, int CM1, typename XT = T, int CPT = 1>
+__global__ void __launch_bounds__(288, MINB)
+    k_mf_q1_stream(MfView<T, 3> A, MfStream G, const XT* __restrict__ x, Epi epi, const T* st0, const T* st1,
+                   double* ws, unsigned* counter, double* red_out, unsigned* kerr) {
+  mf_stream_body<T, Epi, NST, TY, CM1, XT, 8, CPT>(A, G, x, epi, st0, st1, ws, counter, red_out, kerr);
+}
+
+// 16 consumer warps: one CTA per SM (544 threads; registers go to warps in groups of four, so the
+// block is charged as 20 warps, 96 registers each)
+template<typename T, typename Epi, int NST, int TY, int CM1, typename XT = T, int CPT = 1>
+__global__ void __launch_bounds__(544, 1)
+    k_mf_q1_stream16(MfView<T, 3> A, MfStream G, const XT* __restrict__ x, Epi epi, const T* st0, const T* st1,
+                     double* ws, unsigned* counter, double* red_out, unsigned* kerr) {
+  mf_stream_body<T, Epi, NST, TY, CM1, XT, 16, CPT>(A, G, x, epi, st0, st1, ws, counter, red_out, kerr);
+}
+
+// 12 consumer warps: one CTA per SM (416 threads, charged as 16 warps: 128 registers each), for the
+// two-rows-per-thread form
+template<typename T, typename Epi, int NST, int TY, int CM1, typename XT = T, int CPT = 1>
+__global__ void __maxnreg__(128)
+    k_mf_q1_stream12(MfView<T, 3> A, MfStream G, const XT* __restrict__ x, Epi epi, const T* st0, const T* st1,
+                     double* ws, unsigned* counter, double* red_out, unsigned* kerr) {
+  mf_stream_body<T, Epi, NST, TY, CM1, XT, 12, CPT>(A, G, x, epi, st0, st1, ws, counter, red_out, kerr);
 }
 
 }  // namespace fb

@@ -574,17 +574,19 @@ static int launch_mf_tiled_ty(fb_mg* m, const Level& L, const MfView<T, 3>& v, c
 }
 
 // streaming launch (levels of 257^3 and 129^3 points, filter = the lattice boundary): NST stages of
-// TY lines, two CTAs per SM; one contiguous range of slab-lines per CTA
-template<typename T, typename Epi, int TY, int NST, int CM1, typename XT = T, int NCW = 8, int MINB = 2>
+// TY lines, NCW consumer warps per CTA (8: MINB CTAs per SM; 12 or 16: one), CPT rows per thread;
+// one contiguous range of slab-lines per CTA
+template<typename T, typename Epi, int TY, int NST, int CM1, typename XT = T, int NCW = 8, int MINB = 2, int CPT = 1>
 static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, const XT* x, const Epi& epi,
                             double* red_out) {
   using SE = Staged<Epi>;
   constexpr int NS = SE::kStreams;
   constexpr uint32_t M1 = CM1, N = M1 - 1, W = M1 - 2;
   constexpr int NT = 32 * (NCW + 1);
+  constexpr uint32_t PW = (W + CPT - 1) / CPT;  // consumer threads per line
   auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
   MfStream G{};
-  G.G = std::max<uint32_t>(1, uint32_t(32 * NCW) / W);
+  G.G = std::max<uint32_t>(1, uint32_t(32 * NCW) / PW);
   G.nslab = (W + G.G - 1) / G.G;
   G.units = uint64_t(G.nslab) * W;
   G.cap_x = r16(uint64_t(TY) * M1 * sizeof(XT)) + 32;
@@ -596,7 +598,11 @@ static int launch_mf_stream(fb_mg* m, const Level& L, const MfView<T, 3>& v, con
   G.direct_masked = (L.mask && SE::mask(epi) == L.mask) ? 1u : 0u;
   G.inject = m->inject;
   const size_t dyn = size_t(NST) * G.stage_bytes;
-  auto fn = k_mf_q1_stream<T, Epi, NST, MINB, TY, CM1, XT, NCW>;
+  static_assert(NCW == 8 || NCW == 12 || NCW == 16, "8, 12 or 16 consumer warps");
+  void (*fn)(MfView<T, 3>, MfStream, const XT*, Epi, const T*, const T*, double*, unsigned*, double*, unsigned*);
+  if constexpr (NCW == 8) fn = k_mf_q1_stream<T, Epi, NST, MINB, TY, CM1, XT, CPT>;
+  else if constexpr (NCW == 12) fn = k_mf_q1_stream12<T, Epi, NST, TY, CM1, XT, CPT>;
+  else fn = k_mf_q1_stream16<T, Epi, NST, TY, CM1, XT, CPT>;
   static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
   if (dyn > attr) {
     FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
@@ -654,9 +660,17 @@ static int launch_mf_tiled(fb_mg* m, const Level& L, const MfView<T, 3>& v, cons
                          std::is_same<Epi, EpiJacobiK<float, false, true>>::value) ? 7 : TY;
   if constexpr (std::is_same<T, float>::value && std::is_same<XT, float>::value) {
     if (stream_ok<T, Epi, XT>(m, L, epi)) {
-      // 257^3: one CTA of 16 consumer warps per SM (slabs of two planes share their x planes), 4
-      // stages of 6 lines (3 with two streamed vectors): 15.21 against 15.40 ms with two CTAs of 8
-      // warps, same box; 129^3: two CTAs of 8 warps, 3 stages (14.5 against 16.2 us per launch)
+      // 257^3, at most one streamed vector: one CTA of 12 consumer warps per SM, two adjacent rows
+      // per thread (slabs of three planes), 3 stages of 6 lines: Jacobi step 64.0 us, defect 60.8
+      // us per launch, solve 14.57 ms (with the boundary rows left out of both forms, 61.6 against
+      // 64.5 us per Jacobi step with one row per thread and 16 warps). Two streamed vectors: one
+      // CTA of 16 warps, one row per thread (slabs of two planes share their x planes), 3 stages
+      // (one CTA of 16 warps with 4 stages ran the solve in 15.21 against 15.40 ms with two CTAs
+      // of 8 warps, same box). 129^3: two CTAs of 8 warps, 3 stages (14.5 against 16.2 us per
+      // launch)
+      if constexpr (Staged<Epi>::kStreams <= 1) {
+        if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, 3, 257, XT, 12, 1, 2>(m, L, v, x, epi, red_out);
+      }
       constexpr int NSTW = Staged<Epi>::kStreams > 1 ? 3 : 4;
       if (L.M1 == 257) return launch_mf_stream<T, Epi, 6, NSTW, 257, XT, 16, 1>(m, L, v, x, epi, red_out);
       return launch_mf_stream<T, Epi, 6, 3, 129, XT>(m, L, v, x, epi, red_out);

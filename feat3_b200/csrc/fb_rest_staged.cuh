@@ -82,28 +82,12 @@ __global__ void __launch_bounds__(288, 1) k_rest_q1_staged(MfTile G, uint32_t Mf
     __syncwarp();
   } else {
     // ---------------- coarse boundary rows (filtered: zero), while the first copies fly
-    {
-      const uint32_t cpl = (Mc1 + 31) / 32;  // chunks per boundary line
-      const uint32_t nitems = G.nbl_items + G.nedge_items;
-      for (uint32_t item = blockIdx.x * 8 + warp; item < nitems; item += gridDim.x * 8) {
-        int32_t row = -1;
-        if (item < G.nbl_items) {
-          const uint32_t bl = item / cpl;
-          const uint32_t X = (item - bl * cpl) * 32 + lane;
-          uint32_t Y, Z;
-          if (bl < 2 * Mc1) { Z = bl < Mc1 ? 0 : Mc1 - 1; Y = bl < Mc1 ? bl : bl - Mc1; }
-          else { const uint32_t r = bl - 2 * Mc1; Z = 1 + (r >> 1); Y = (r & 1) ? Mc1 - 1 : 0; }
-          if (X < Mc1) row = int32_t((Z * Mc1 + Y) * Mc1 + X);
-        } else {
-          const uint32_t li = (item - G.nbl_items) * 16 + (lane >> 1);
-          if (li < Wc * Wc) {
-            const uint32_t zq = li / Wc;
-            const uint32_t Y = 1 + (li - zq * Wc), Z = 1 + zq;
-            const uint32_t X = (lane & 1) ? Mc1 - 1 : 0;
-            row = int32_t((Z * Mc1 + Y) * Mc1 + X);
-          }
-        }
-        if (row >= 0) acc += epi(uint32_t(row), T(0));
+    for (uint32_t item = blockIdx.x * 8 + warp; item < G.nbl_items + G.nedge_items; item += gridDim.x * 8) {
+      uint32_t X, Y, Z;
+      const int32_t row = direct_row(item, lane, Mc1, G.nbl_items, X, Y, Z);
+      if (row >= 0) {
+        epi.rhs[row] = T(0);
+        if (epi.sol1) epi.sol1[row] = T(0);
       }
     }
     // ---------------- consumers: TYC coarse rows per thread and tile
