@@ -1844,7 +1844,8 @@ int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (!m || !c) return FB_ERR_INVALID;
   if (c->nu < 1 || c->nu > 64 || c->max_iter < 0 || !(c->tol_rel >= 0.0) ||
       c->precision < 0 || c->precision > 2 || c->outer < 0 || c->outer > 1 || c->coarse < 0 || c->coarse > 3 ||
-      c->format < 0 || c->format > 2 || c->cycle < 0 || c->cycle > 2 || c->adapt_cgc < 0 || c->adapt_cgc > 2)
+      c->format < 0 || c->format > 2 || c->cycle < 0 || c->cycle > 2 || c->adapt_cgc < 0 || c->adapt_cgc > 2 ||
+      (c->flags & ~15))
     return FB_ERR_INVALID;
   if (c->coarse == FB_COARSE_PCG && !m->coarse_csr.rp) return FB_ERR_UNSUPPORTED;
   if (c->coarse == FB_COARSE_DIRECT && !m->cinv64) return FB_ERR_UNSUPPORTED;

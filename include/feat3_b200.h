@@ -275,7 +275,8 @@ typedef struct fb_solver_cfg {
   int precision;
   int use_graphs;     /* capture the per-iteration launch sequence in a CUDA graph */
   int format;         /* FB_FORMAT_SELL, FB_FORMAT_STENCIL or FB_FORMAT_MATFREE */
-  int flags;          /* FB_FLAG_*: switch individual fusions off (testing; 0 = all on) */
+  int flags;          /* FB_FLAG_*: switch individual fusions off (testing; 0 = all on; any other
+                         bit: FB_ERR_INVALID) */
   int cycle;          /* FB_CYCLE_V, FB_CYCLE_F or FB_CYCLE_W (Solver::MultiGridCycle) */
   int adapt_cgc;      /* FB_CGC_FIXED, FB_CGC_MIN_ENERGY or FB_CGC_MIN_DEFECT (Solver::MultiGridAdaptCGC) */
 } fb_solver_cfg;

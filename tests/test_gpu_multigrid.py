@@ -286,3 +286,19 @@ def test_stream_kernel_matches_tiled(lvl):
     assert s1["status"] == s2["status"] == "success" and s1["iters"] == s2["iters"]
     assert relerr(s1["u"].cpu().numpy(), s2["u"].cpu().numpy()) <= 1e-12
     mg.close()
+
+
+def test_unknown_flags_are_rejected():
+    """fb_mg_configure refuses flag bits it does not define (FB_ERR_INVALID), and keeps the previous
+    configuration usable"""
+    import ctypes
+    from feat3_b200 import _lib
+    from feat3_b200.solver import MultiGrid
+    mg = MultiGrid.structured(3, 1, 3, 1).configure(nu=2, format="matfree")
+    cfg = _lib.SolverCfg()
+    _lib.load().fb_solver_cfg_default(ctypes.byref(cfg))
+    for bad in (16, 1 << 20, -1):
+        cfg.flags = bad
+        assert _lib.load().fb_mg_configure(mg.h, ctypes.byref(cfg)) == _lib.FB_ERR_INVALID
+    assert mg.solve(mg.assemble_rhs("one"))["status"] == "success"
+    mg.close()
