@@ -37,7 +37,6 @@ struct CoarseArgs {
   int nlv, nu, coarse;
   T omega;
   const T* cinv;            // dense inverse of the coarsest filtered system (FB_COARSE_DIRECT)
-  double* red;              // 2 x 32 doubles of reduction scratch
   int s1_coarsest;          // the restriction onto the coarsest level forms its first smoothing step
 };
 
@@ -164,15 +163,21 @@ __device__ __forceinline__ T post_row(const CLevel<T>& L, T om, const T* cur, co
   return om * (__ldg(L.invd + i) * d) + xc;
 }
 
-// deterministic cluster-wide sum; ends with a cluster barrier, result in every thread
+// deterministic cluster-wide sum; ends with a cluster barrier, result in every thread. Each CTA
+// stores its partial into slot [its rank] of every CTA's shared array part (distributed shared
+// memory), so after the barrier the partials are summed in rank order from local shared memory.
+// part is double-buffered by the caller (consecutive sums use alternate halves), so a CTA that
+// runs ahead into the next sum never overwrites a partial that a slower CTA has still to read.
 template<int THREADS>
-__device__ __forceinline__ double cluster_sum(double v, double* scratch, double* sh,
+__device__ __forceinline__ double cluster_sum(double v, double* part, double* sh,
                                               cooperative_groups::cluster_group& cl) {
   const double blk = block_sum<THREADS>(v, sh);
-  if (threadIdx.x == 0) __stcg(scratch + cl.block_rank(), blk);
+  const uint32_t nb = cl.num_blocks(), me = cl.block_rank();
+  if (threadIdx.x == 0)
+    for (uint32_t r = 0; r < nb; ++r) *cl.map_shared_rank(part + me, r) = blk;
   cl.sync();
   double t = 0.0;
-  for (uint32_t r = 0; r < cl.num_blocks(); ++r) t += __ldcg(scratch + r);
+  for (uint32_t r = 0; r < nb; ++r) t += part[r];
   return t;
 }
 
@@ -184,6 +189,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
   pdl_trigger();
   cgr::cluster_group cl = cgr::this_cluster();
   __shared__ double sh[THREADS / 32];
+  __shared__ double part[2][16];  // cluster partials, double-buffered
   const uint32_t gt = cl.block_rank() * THREADS + threadIdx.x;
   const uint32_t gs = cl.num_blocks() * THREADS;
   const int nu = A.nu;
@@ -228,7 +234,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
       if (s1) C.x[i] = mk ? T(0) : om * (__ldg(C.invd + i) * v);
       acc += double(v) * double(v);
     }
-    bnorm = cluster_sum<THREADS>(acc, A.red + 32 * (rk++ & 1), sh, cl);
+    bnorm = cluster_sum<THREADS>(acc, part[rk++ & 1], sh, cl);
     if (gt == 0) *C.bn = bnorm;
   }
   // ---------------- coarsest level (multigrid.hpp:1524-1587)
@@ -299,7 +305,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
         oth[i] = post_row(L, om, cur, b, s0, i, s, skip, it == 0, acc);
       }
       if (it == 0) {
-        dn = cluster_sum<THREADS>(acc, A.red + 32 * (rk++ & 1), sh, cl);
+        dn = cluster_sum<THREADS>(acc, part[rk++ & 1], sh, cl);
         if (gt == 0) *L.dn = dn;
         if (nu == 1) {
           // the smoother skipped: its result is the prolongated iterate (k_skip_fix)

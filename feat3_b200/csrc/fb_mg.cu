@@ -776,9 +776,8 @@ static int spmv_L(fb_mg* m, const Level& L, const T* x, const Epi& epi, double* 
 
 // bulk-staged 3D restriction onto a coarse level whose filter is its lattice boundary: tiles of
 // TYC coarse lines per thread group, 2-deep ring, as many CTAs as fit (2 per SM at 129^3)
-template<typename T, int TYC>
+template<typename T, int TYC, int NST = 2>
 static int launch_rest_staged(fb_mg* m, const Level& L, const T* xf, const EpiRestrict<T>& epi, double* red) {
-  constexpr int NST = 2;
   const uint32_t Mc1 = L.tr.Mc1, Mf1 = L.tr.Mf1, Wc = Mc1 - 2;
   MfTile G{};
   G.M1 = Mc1; G.N = Mc1 - 1;
@@ -969,7 +968,6 @@ static int launch_coarse(fb_mg* m, int lc, T** sol_lc) {
   A.coarse = m->cfg.coarse;
   A.omega = T(m->cfg.omega_rich);
   if constexpr (std::is_same<T, double>::value) A.cinv = m->cinv64; else A.cinv = m->cinv32;
-  A.red = m->cred;
   A.s1_coarsest = m->cfg.coarse == FB_COARSE_SMOOTHER ? 1 : 0;
   for (int i = 0; i < A.nlv; ++i) {
     Level& L = m->L[lc + i];
@@ -1683,7 +1681,6 @@ int common_init(fb_mg* m) {
   FB_CUDA(cudaMemsetAsync(m->dbg_err, 0, sizeof(unsigned long long), m->stream));
   m->kerr = &m->sc->kerr;
   m->inject = &m->sc->inject;
-  FB_TRY(dalloc(m, &m->cred, 64));
   FB_CUDA(cudaStreamSynchronize(m->stream));
   FB_CUDA(cudaMallocHost(&m->host_rr, sizeof(double) * 4));
   FB_CUDA(cudaEventCreate(&m->ev0));

@@ -150,12 +150,11 @@ struct fb_mg {
   int g_body_key = -1;
   int launches = 0;
   int body_launches = 0;
-  bool top_s1 = false;
+  bool top_s1 = false;                   // finest-level first smoothing step already formed (fused)
   bool top_dot = false;                  // the V-cycle's last finest-level step also forms r . z
   unsigned long long* dbg_err = nullptr;  // FB_DEBUG=1: device word for kernel self-checks
   unsigned* kerr = nullptr;               // &sc->kerr: set by a staged kernel whose bounded wait expired
   unsigned* inject = nullptr;             // &sc->inject (test hook)
-  double* cred = nullptr;                 // reduction scratch of the fused coarse cycle (2 x 32)                   // finest-level first smoothing step already formed (fused)
   double *hb = nullptr, *hx = nullptr;   // staging for the host-buffer solve
   double* adj = nullptr;                 // adjoint right-hand side
   // FEAT numbering at the C-ABI (structured hierarchies created with FB_NUMBERING_FEAT):
