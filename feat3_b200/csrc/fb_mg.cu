@@ -124,13 +124,27 @@ static int launch_stencil_S(fb_mg* m, const DevStencil& St, const void* val, flo
   return FB_OK;
 }
 
+// the stored offsets are those of a lattice of M1 points per side (lattice_off)
+template<int S, int CM1>
+static bool offsets_are(const DevStencil& St, uint32_t M1) {
+  if (M1 != uint32_t(CM1)) return false;
+  for (int j = 0; j < S; ++j)
+    if (St.off[j] != lattice_off<S, CM1>(j)) return false;
+  return true;
+}
+
+// levels of 257^3 and 129^3 points take the lattice size as a compile-time constant
 template<typename VT, typename Epi, int S>
 static int launch_stencil_packed_S(fb_mg* m, const DevStencil& St, const void* val, float scale, uint32_t rows,
-                                   const float* x, const Epi& epi, double* red_out) {
+                                   uint32_t M1, const float* x, const Epi& epi, double* red_out) {
   StencilView<S> v;
   v.rows = rows; v.nchunks = St.nchunks; v.val = val; v.scale = scale;
   for (int j = 0; j < S; ++j) v.off[j] = St.off[j];
   auto fn = k_stencil_packed<VT, Epi, S>;
+  if constexpr (S == 27) {
+    if (offsets_are<S, 257>(St, M1)) fn = k_stencil_packed<VT, Epi, S, 257>;
+    else if (offsets_are<S, 129>(St, M1)) fn = k_stencil_packed<VT, Epi, S, 129>;
+  }
   fn<<<occupancy_grid((const void*)fn, St.nchunks), 256, 0, m->stream>>>(v, x, epi, m->ws, m->counter, red_out);
   m->launches++;
   FB_CHECK_LAUNCH();
@@ -144,8 +158,8 @@ static int launch_stencil(fb_mg* m, const Level& L, int prec, const XT* x, const
     // 2- and 4-byte values use the packed layout (8-byte loads per lane)
     const float scale = prec == FB_PREC_F16 ? St.scale16 : 1.0f;
     const void* pv = prec == FB_PREC_F16 ? (const void*)St.v16 : (const void*)St.v32;
-    if (St.S == 27) return launch_stencil_packed_S<VT, Epi, 27>(m, St, pv, scale, L.n, x, epi, red_out);
-    if (St.S == 9) return launch_stencil_packed_S<VT, Epi, 9>(m, St, pv, scale, L.n, x, epi, red_out);
+    if (St.S == 27) return launch_stencil_packed_S<VT, Epi, 27>(m, St, pv, scale, L.n, L.M1, x, epi, red_out);
+    if (St.S == 9) return launch_stencil_packed_S<VT, Epi, 9>(m, St, pv, scale, L.n, L.M1, x, epi, red_out);
     return FB_ERR_UNSUPPORTED;
   }
   const void* val = prec == FB_PREC_F64 ? (const void*)St.v64 : (prec == FB_PREC_F32 ? (const void*)St.v32 : (const void*)St.v16);

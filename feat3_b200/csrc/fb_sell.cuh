@@ -357,7 +357,17 @@ template<> struct Pack8<float> {
   }
 };
 
-template<typename VT, typename Epi, int S>
+// slot j's neighbour offset on a lattice of CM1 points per side (slot j = (dz+1)*9 + (dy+1)*3 +
+// (dx+1) in 3D, (dy+1)*3 + (dx+1) in 2D): a compile-time constant, so that the gathers of a chunk
+// whose neighbours all lie inside the vector take it as an immediate address offset
+template<int S, int CM1>
+__host__ __device__ constexpr int32_t lattice_off(int j) {
+  return S == 27 ? ((j / 9 - 1) * CM1 + (j / 3 % 3 - 1)) * CM1 + (j % 3 - 1) : (j / 3 - 1) * CM1 + (j % 3 - 1);
+}
+
+// CM1 > 0: the lattice size as a compile-time constant (the launcher checks that the stored
+// offsets are those of lattice_off); 0: offsets from the view
+template<typename VT, typename Epi, int S, int CM1 = 0>
 __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, const float* __restrict__ x, Epi epi,
                                                            double* ws, unsigned* counter, double* red_out) {
   constexpr int W = Pack8<VT>::W;
@@ -367,24 +377,40 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
   const uint32_t wpb = blockDim.x >> 5;
   const VT* __restrict__ val = static_cast<const VT*>(A.val);
   const int32_t last = int32_t(A.rows) - 1;
+  auto off = [&](int j) -> int32_t {
+    if constexpr (CM1 > 0) return lattice_off<S, CM1>(j);
+    else return A.off[j];
+  };
   double acc = 0.0;
   for (uint32_t c = blockIdx.x * wpb + (threadIdx.x >> 5); c < A.nchunks; c += gridDim.x * wpb) {
     const int32_t row0 = int32_t(c) * 32;
     const int32_t row = row0 + lane;
     const VT* vp = val + (size_t(c) * G * 32 + lane) * W;
-    const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
+    const bool inside = row0 + off(0) >= 0 && row0 + 31 + off(S - 1) <= last;
     float sum = 0.0f;
+    if (inside) {
+      const float* xr = x + row;
 #pragma unroll
-    for (int g = 0; g < G; ++g) {
-      float v[W];
-      Pack8<VT>::ld(vp + g * 32 * W, v);
+      for (int g = 0; g < G; ++g) {
+        float v[W];
+        Pack8<VT>::ld(vp + g * 32 * W, v);
 #pragma unroll
-      for (int e = 0; e < W; ++e) {
-        const int j = g * W + e;
-        if (j < S) {
-          int32_t col = row + A.off[j];
-          if (!inside) col = col < 0 ? 0 : (col > last ? last : col);
-          sum += v[e] * __ldg(x + col);
+        for (int e = 0; e < W; ++e)
+          if (g * W + e < S) sum += v[e] * __ldg(xr + off(g * W + e));
+      }
+    } else {
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        float v[W];
+        Pack8<VT>::ld(vp + g * 32 * W, v);
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+          const int j = g * W + e;
+          if (j < S) {
+            int32_t col = row + off(j);
+            col = col < 0 ? 0 : (col > last ? last : col);
+            sum += v[e] * __ldg(x + col);
+          }
         }
       }
     }
