@@ -18,6 +18,7 @@
 #include "fb_mg_internal.cuh"
 #include "fb_mf.cuh"
 #include "fb_mf_stream.cuh"
+#include "fb_stencil_stream.cuh"
 #include "fb_rest_staged.cuh"
 #include "fb_coarse.cuh"
 
@@ -151,6 +152,48 @@ static int launch_stencil_packed_S(fb_mg* m, const DevStencil& St, const void* v
   return FB_OK;
 }
 
+// the streaming stencil SpMV on the 257^3 level (x staged once per run, register window): one CTA
+// of 16 consumer warps per SM (slabs of two planes), 4 stages of 6 lines (FP16 values)
+template<typename VT, typename Epi>
+static int launch_stencil_stream(fb_mg* m, const void* val, float scale, const float* x, const Epi& epi,
+                                 double* red_out) {
+  using SE = Staged<Epi>;
+  constexpr int NS = SE::kStreams, NCW = 16, TY = 6, NST = 4, NT = 32 * (NCW + 1);
+  constexpr uint32_t M1 = 257, W = M1 - 2;
+  auto r16 = [](uint64_t b) { return uint32_t((b + 15) & ~uint64_t(15)); };
+  StStream G{};
+  G.G = std::max<uint32_t>(1, uint32_t(32 * NCW) / W);
+  G.nslab = (W + G.G - 1) / G.G;
+  G.units = uint64_t(G.nslab) * W;
+  G.cap_x = r16(uint64_t(TY) * M1 * sizeof(float)) + 32;
+  G.cap_s = NS ? r16(uint64_t(TY) * M1 * sizeof(float)) + 32 : 0;
+  G.stage_bytes = ((G.G + 2) * G.cap_x + NS * G.G * G.cap_s + 127) & ~127u;
+  G.nbl_items = (4 * M1 - 4) * ((M1 + 31) / 32);
+  G.nedge_items = (W * W + 15) / 16;
+  G.scale = scale;
+  G.inject = m->inject;
+  const size_t dyn = size_t(NST) * G.stage_bytes;
+  auto fn = k_stencil_stream<VT, Epi, NST, TY, 257, NCW>;
+  static size_t attr = 0;  // per instantiation: largest dynamic shared memory requested so far
+  if (dyn > attr) {
+    FB_CUDA(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+    attr = dyn;
+  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, (const void*)fn, NT, dyn) != cudaSuccess || bps < 1) {
+    cudaGetLastError();
+    bps = 1;
+  }
+  const uint32_t grid = uint32_t(std::min<uint64_t>(G.units, uint64_t(bps) * kSMs));
+  const float* s0 = NS > 0 ? static_cast<const float*>(SE::stream(epi, 0)) : nullptr;
+  const float* s1 = NS > 1 ? static_cast<const float*>(SE::stream(epi, 1)) : nullptr;
+  FB_CUDA(launch_pdl(m->stream, fn, dim3(grid), dim3(NT), dyn, G, static_cast<const VT*>(val), x, epi, s0, s1, m->ws,
+                     m->counter, red_out, m->kerr));
+  m->launches++;
+  FB_CHECK_LAUNCH();
+  return FB_OK;
+}
+
 template<typename VT, typename XT, typename AT, typename Epi>
 static int launch_stencil(fb_mg* m, const Level& L, int prec, const XT* x, const Epi& epi, double* red_out) {
   const DevStencil& St = L.St;
@@ -158,6 +201,14 @@ static int launch_stencil(fb_mg* m, const Level& L, int prec, const XT* x, const
     // 2- and 4-byte values use the packed layout (8-byte loads per lane)
     const float scale = prec == FB_PREC_F16 ? St.scale16 : 1.0f;
     const void* pv = prec == FB_PREC_F16 ? (const void*)St.v16 : (const void*)St.v32;
+    if constexpr (Staged<Epi>::kOk && std::is_same<XT, float>::value && std::is_same<VT, __half>::value) {
+      // FP16 values at 257^3 with the lattice boundary as the filter: the streaming form (246
+      // against 294 us per Jacobi step, FP16-stencil mixed solve 43.5 against 46.8 ms; with FP32
+      // values, 14 value loads per row, it ran slower: 396 against 364 us)
+      if (St.S == 27 && offsets_are<27, 257>(St, L.M1) && L.mask_boundary && L.mask &&
+          Staged<Epi>::mask(epi) == L.mask && Staged<Epi>::input_is_x(epi, x) && !(m->cfg.flags & FB_FLAG_NO_STREAM))
+        return launch_stencil_stream<VT, Epi>(m, pv, scale, x, epi, red_out);
+    }
     if (St.S == 27) return launch_stencil_packed_S<VT, Epi, 27>(m, St, pv, scale, L.n, L.M1, x, epi, red_out);
     if (St.S == 9) return launch_stencil_packed_S<VT, Epi, 9>(m, St, pv, scale, L.n, L.M1, x, epi, red_out);
     return FB_ERR_UNSUPPORTED;

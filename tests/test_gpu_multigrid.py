@@ -317,3 +317,25 @@ def test_coarse_cluster_matches_level_kernels(dim, lvl, prec):
     b = mg.configure(nu=2, precision=prec, format="matfree", fuse_coarse=False).vcycle(d).cpu().numpy()
     np.testing.assert_array_equal(a, b)
     mg.close()
+
+
+@pytest.mark.parametrize("prec", ["f16", "f32"])
+def test_stencil_stream_matches_packed(prec):
+    """the streaming stencil SpMV of the 257^3 level (x staged once per run, register window; FP16
+    values) sums each row's 27 products in the packed kernel's slot order: one V-cycle on the FP16
+    stencil values is bit-identical with either kernel (FP32 values take the packed kernel either
+    way); mixed PCG solves (whose r . z groups its partial sums differently) take the same
+    iterations and agree to rounding"""
+    from feat3_b200.solver import MultiGrid
+    k = lognormal_k(3, 8, 1.0, seed=23)
+    mg = MultiGrid.structured(3, 1, 8, 1, k)
+    d = mg.assemble_rhs("one")
+    common = dict(nu=2, precision=prec, format="stencil")
+    a = mg.configure(**common).vcycle(d).cpu().numpy()
+    b = mg.configure(stream=False, **common).vcycle(d).cpu().numpy()
+    np.testing.assert_array_equal(a, b)
+    s1 = mg.configure(**common).solve(d)
+    s2 = mg.configure(stream=False, **common).solve(d)
+    assert s1["status"] == s2["status"] == "success" and s1["iters"] == s2["iters"]
+    assert relerr(s1["u"].cpu().numpy(), s2["u"].cpu().numpy()) <= 1e-12
+    mg.close()
