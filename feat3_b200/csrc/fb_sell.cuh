@@ -101,21 +101,23 @@ struct EpiJacobi {
   const T* x; const T* rhs; const T* invd; T* out; const T* s0; const uint32_t* mask;
   const double* skip_src; T omega;
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
+    // every input is loaded before out is stored (a load after the store would wait behind it)
+    const T b = rhs[row];
     if (smoother_skip<T>(skip_src)) {
       const T o = s0 ? s0[row] : T(0);
       out[row] = o;
-      return DOT ? double(o) * double(rhs[row]) : 0.0;
+      return DOT ? double(o) * double(b) : 0.0;
     }
-    const T d = rhs[row] - s;
+    const T d = b - s;
     if (masked(mask, row)) {
       const T o = x[row];
       out[row] = o;
-      return DOT ? double(o) * double(rhs[row]) : 0.0;
+      return DOT ? double(o) * double(b) : 0.0;
     }
     const T t = invd[row] * d;
     const T o = omega * t + x[row];
     out[row] = o;
-    return RED ? double(d) * double(d) : (DOT ? double(o) * double(rhs[row]) : 0.0);
+    return RED ? double(d) * double(d) : (DOT ? double(o) * double(b) : 0.0);
   }
 };
 
@@ -137,8 +139,11 @@ struct EpiPcgQ {
   T* q; const PT* p; const uint32_t* mask;
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
     const T v = masked(mask, row) ? T(0) : s;
+    // p's value is loaded before q is stored: a load after the store could not be moved ahead
+    // of it (q might alias p as far as the compiler knows) and would wait behind it
+    const PT pr = __ldg(p + row);
     q[row] = v;
-    return double(v) * double(p[row]);
+    return double(v) * double(pr);
   }
 };
 
@@ -151,8 +156,9 @@ struct EpiRestrict {
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
     const bool m = masked(mask, row);
     const T v = m ? T(0) : s;
+    const T id = sol1 ? __ldg(invd + row) : T(0);  // loaded before the stores (as in EpiPcgQ)
     rhs[row] = v;
-    if (sol1) sol1[row] = m ? T(0) : omega * (invd[row] * v);
+    if (sol1) sol1[row] = m ? T(0) : omega * (id * v);
     return double(v) * double(v);
   }
 };
