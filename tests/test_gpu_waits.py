@@ -62,3 +62,22 @@ def test_expired_wait_in_the_streaming_kernel():
     after = mg.vcycle(d).cpu().numpy()
     np.testing.assert_array_equal(after, before)
     mg.close()
+
+
+def test_expired_wait_in_the_stencil_stream_kernel():
+    """the same through the streaming FP16 stencil SpMV of the 257^3 level: one V-cycle on the
+    FP16 stencil values, whose first staged launch is that kernel's smoothing step, returns
+    FB_ERR_TIMEOUT, and the next one on the same handle is bit-identical to one before the expiry"""
+    from feat3_b200 import _lib
+    from feat3_b200.solver import MultiGrid
+    k = np.exp(np.random.default_rng(35).standard_normal(256 ** 3))
+    mg = MultiGrid.structured(3, 1, 8, 1, k).configure(nu=2, precision="f16", format="stencil")
+    d = mg.assemble_rhs("one")
+    before = mg.vcycle(d).cpu().numpy()
+    _lib.call("fb_mg_test_expire_wait", mg.h)
+    with pytest.raises(_lib.FeatError) as err:
+        mg.vcycle(d)
+    assert err.value.code == FB_ERR_TIMEOUT
+    after = mg.vcycle(d).cpu().numpy()
+    np.testing.assert_array_equal(after, before)
+    mg.close()
