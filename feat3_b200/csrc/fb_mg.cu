@@ -325,9 +325,9 @@ template<> struct Pair<float> { using type = float2; };
 template<> struct Pair<double> { using type = double2; };
 
 template<bool LOW>
-// The x update x += alpha p of this step is deferred to the next k_pcg_dir, which reads p
-// anyway before overwriting it (or to k_pcg_finish after the last iteration): the same
-// operation on the same values, one pass over p fewer per iteration. Two rows per thread and
+// The x update x += alpha p of this step is deferred to a later k_pcg_dir2, which reads p
+// anyway (or to k_pcg_finish2 after the last iteration): the same operation on the same values,
+// fewer passes over p and x. Two rows per thread and
 // step, with 8- and 16-byte accesses (all vectors are allocation bases, so pairs are aligned).
 __global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const double* __restrict__ q,
                                                     DevScalars* sc, uint32_t n, double* ws, unsigned* counter,
@@ -386,15 +386,6 @@ __global__ void __launch_bounds__(256) k_pcg_update(double* r, float* r32, const
   }
 }
 
-// the x update of the last PCG step (pcg.hpp:256)
-template<typename PT>
-__global__ void k_pcg_finish(double* x, const PT* __restrict__ p, const DevScalars* sc, uint32_t n) {
-  const double alpha = sc->alpha;
-  if (alpha == 0.0) return;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] = alpha * double(p[i]) + x[i];
-}
-
 // r . z with z in FP64 or FP32 (ConvertPrecond: z = double(z_inner))
 template<typename ZT>
 __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, const ZT* __restrict__ z, uint32_t n,
@@ -410,45 +401,83 @@ __global__ void __launch_bounds__(256) k_dot_rz(const double* __restrict__ r, co
 }
 
 // p = z + beta p, beta = rz / gamma (pcg.hpp:275-282); gamma <- rz is committed by k_pcg_update.
-// First the previous step's pending x += alpha p (pcg.hpp:256), on the old p. PT = float: the
-// direction is stored rounded to FP32 (the mixed matrix-free form); q = A p, x += alpha p and
-// q . p then all use the stored direction, so r stays the defect of x, and only the conjugacy
-// of successive directions carries the FP32 rounding, below that of the FP32 preconditioner.
-template<typename ZT, typename PT = double>
-__global__ void k_pcg_dir(PT* p, double* x, const ZT* __restrict__ z, const DevScalars* sc, uint32_t n) {
+// PT = float: the direction is stored rounded to FP32 (the mixed matrix-free form); q = A p,
+// x += alpha p and q . p then all use the stored direction, so r stays the defect of x, and only
+// the conjugacy of successive directions carries the FP32 rounding, below that of the FP32
+// preconditioner. The pending x updates (pcg.hpp:256) are deferred over two iterations:
+// iteration j writes p_j into the buffer j & 1 (pout), from p_{j-1} in the other one (pin). An even
+// j (HOLD) does not touch x: it holds alpha_{j-1} (sc->alpha_hold), whose direction p_{j-1} stays
+// in pin. An odd j applies both pending steps in their order, x += alpha_{j-2} p_{j-2} (held, read
+// from pout before it is overwritten), then x += alpha_{j-1} p_{j-1}: the x updates of PCG on the
+// same values in the same order, with one read and one write of x per two iterations.
+template<typename ZT, typename PT, bool HOLD>
+__global__ void k_pcg_dir2(PT* pout, const PT* __restrict__ pin, double* x, const ZT* __restrict__ z, DevScalars* sc,
+                           uint32_t n) {
   using P2 = typename Pair<PT>::type;
   using Z2 = typename Pair<ZT>::type;
   pdl_wait();
   const double beta = sc->rz / sc->gamma;
   const bool upd = fabs(beta) >= eps_of<double>();
-  const double alpha = sc->alpha;
-  const bool xup = alpha != 0.0;
+  const double a1 = HOLD ? 0.0 : sc->alpha_hold, a2 = HOLD ? 0.0 : sc->alpha;
+  const bool x1 = a1 != 0.0, x2 = a2 != 0.0;
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  // two rows per thread and step (allocation bases: pairs are aligned)
   for (uint32_t j = tid; j < n / 2; j += stride) {
-    const P2 pv = reinterpret_cast<const P2*>(p)[j];
+    const P2 pv = reinterpret_cast<const P2*>(pin)[j];
     const Z2 zv = __ldg(reinterpret_cast<const Z2*>(z) + j);
     const double p0 = double(pv.x), p1 = double(pv.y);
-    if (xup) {
+    if (!HOLD && (x1 || x2)) {
       double2 xv = reinterpret_cast<const double2*>(x)[j];
-      xv.x = alpha * p0 + xv.x;
-      xv.y = alpha * p1 + xv.y;
+      if (x1) {
+        const P2 hv = reinterpret_cast<const P2*>(pout)[j];
+        xv.x = a1 * double(hv.x) + xv.x;
+        xv.y = a1 * double(hv.y) + xv.y;
+      }
+      if (x2) {
+        xv.x = a2 * p0 + xv.x;
+        xv.y = a2 * p1 + xv.y;
+      }
       reinterpret_cast<double2*>(x)[j] = xv;
     }
     P2 o;
     o.x = PT(upd ? beta * p0 + double(zv.x) : double(zv.x));
     o.y = PT(upd ? beta * p1 + double(zv.y) : double(zv.y));
-    reinterpret_cast<P2*>(p)[j] = o;
+    reinterpret_cast<P2*>(pout)[j] = o;
   }
   if ((n & 1u) && tid == 0) {
     const uint32_t i = n - 1;
-    const double pi = double(p[i]);
-    if (xup) x[i] = alpha * pi + x[i];
-    p[i] = PT(upd ? beta * pi + double(z[i]) : double(z[i]));
+    const double pi = double(pin[i]);
+    if (!HOLD && (x1 || x2)) {
+      double xi = x[i];
+      if (x1) xi = a1 * double(pout[i]) + xi;
+      if (x2) xi = a2 * pi + xi;
+      x[i] = xi;
+    }
+    pout[i] = PT(upd ? beta * pi + double(z[i]) : double(z[i]));
+  }
+  if (HOLD && tid == 0) sc->alpha_hold = sc->alpha;
+}
+
+// the x updates still pending after the last iteration J (pcg.hpp:256): alpha_{J-1} p_{J-1}
+// (held, J even) and alpha_J p_J, in that order
+template<typename PT>
+__global__ void k_pcg_finish2(double* x, const PT* __restrict__ phold, const PT* __restrict__ plast,
+                              const DevScalars* sc, uint32_t n, int use_hold) {
+  const double a1 = use_hold ? sc->alpha_hold : 0.0, a2 = sc->alpha;
+  if (a1 == 0.0 && a2 == 0.0) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double xi = x[i];
+    if (a1 != 0.0) xi = a1 * double(phold[i]) + xi;
+    if (a2 != 0.0) xi = a2 * double(plast[i]) + xi;
+    x[i] = xi;
   }
 }
 
-__global__ void k_init_pcg(DevScalars* sc) { sc->gamma = 1.0; sc->rz = 0.0; sc->alpha = 0.0; }
+__global__ void k_init_pcg(DevScalars* sc) {
+  sc->gamma = 1.0;
+  sc->rz = 0.0;
+  sc->alpha = 0.0;
+  sc->alpha_hold = 0.0;
+}
 
 // adaptive coarse-grid correction factor (multigrid.hpp:1898-1925): MinEnergy
 // omega = (def . cor) / (tmp . cor), MinDefect omega = (def . tmp) / (tmp . tmp), tmp = A cor;
@@ -807,7 +836,7 @@ static bool pcg_p32(const fb_mg* m) {
 }
 
 // q = filter_def(A p) and q . p with p stored in FP32, A(k) in FP64 (finest level)
-static int pcgq_p32(fb_mg* m, double* red) {
+static int pcgq_p32(fb_mg* m, double* red, const float* p) {
   const Level& L = m->L[0];
   MfView<double, 3> v;
   v.rows = L.n; v.nchunks = (L.n + 31) / 32; v.M1 = L.M1; v.ne = L.ne;
@@ -815,8 +844,8 @@ static int pcgq_p32(fb_mg* m, double* red) {
   v.k = L.k;
   for (int r = 0; r < 8; ++r) v.kr[r] = L.kr64[r];
   for (int j = 0; j < 27; ++j) v.off[j] = L.St.off[j];
-  EpiPcgQ<double, float> eq{m->q, m->p32, L.mask};
-  return launch_mf_tiled<double, EpiPcgQ<double, float>, float>(m, L, v, (const float*)m->p32, eq, red);
+  EpiPcgQ<double, float> eq{m->q, p, L.mask};
+  return launch_mf_tiled<double, EpiPcgQ<double, float>, float>(m, L, v, p, eq, red);
 }
 
 // level operator A x with an epilogue, on the storage the configuration selects
@@ -1423,7 +1452,8 @@ static int precond(fb_mg* m, const void** z_out) {
 }
 
 // one outer iteration after a successful stopping test; ends with ||r||^2 copied to the host
-static int body(fb_mg* m) {
+// iteration j (from 1) of the outer solver; PCG's direction buffers alternate with j's parity
+static int body(fb_mg* m, int j) {
   const uint32_t n = m->L[0].n;
   const bool low = m->cfg.precision != FB_PREC_F64;
   const void* z = nullptr;
@@ -1445,19 +1475,35 @@ static int body(fb_mg* m) {
       FB_CHECK_LAUNCH();
     }
     const bool p32 = pcg_p32(m);
-    if (p32) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float, float>, dim3(ew_grid(n)), dim3(256), 0, m->p32, m->xb,
-                                (const float*)z, (const DevScalars*)m->sc, n));
-    else if (low) FB_CUDA(launch_pdl(m->stream, k_pcg_dir<float>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const float*)z,
-                                     (const DevScalars*)m->sc, n));
-    else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir<double>, dim3(ew_grid(n)), dim3(256), 0, m->p, m->xb, (const double*)z,
-                                (const DevScalars*)m->sc, n));
+    const bool odd = (j & 1) != 0;
+    float* pf_out = odd ? m->p32b : m->p32;
+    float* pf_in = odd ? m->p32 : m->p32b;
+    double* pd_out = odd ? m->pb : m->p;
+    double* pd_in = odd ? m->p : m->pb;
+    const dim3 eg(ew_grid(n));
+    if (p32) {
+      if (odd) FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<float, float, false>, eg, dim3(256), 0, pf_out, (const float*)pf_in,
+                                  m->xb, (const float*)z, m->sc, n));
+      else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<float, float, true>, eg, dim3(256), 0, pf_out, (const float*)pf_in,
+                                  m->xb, (const float*)z, m->sc, n));
+    } else if (low) {
+      if (odd) FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<float, double, false>, eg, dim3(256), 0, pd_out,
+                                  (const double*)pd_in, m->xb, (const float*)z, m->sc, n));
+      else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<float, double, true>, eg, dim3(256), 0, pd_out,
+                                  (const double*)pd_in, m->xb, (const float*)z, m->sc, n));
+    } else {
+      if (odd) FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<double, double, false>, eg, dim3(256), 0, pd_out,
+                                  (const double*)pd_in, m->xb, (const double*)z, m->sc, n));
+      else     FB_CUDA(launch_pdl(m->stream, k_pcg_dir2<double, double, true>, eg, dim3(256), 0, pd_out,
+                                  (const double*)pd_in, m->xb, (const double*)z, m->sc, n));
+    }
     m->launches++;
     FB_CHECK_LAUNCH();
     if (p32) {
-      FB_TRY(pcgq_p32(m, &m->sc->qp));
+      FB_TRY(pcgq_p32(m, &m->sc->qp, pf_out));
     } else {
-      EpiPcgQ<double> eq{m->q, m->p, m->L[0].mask};
-      FB_TRY(spmv_L<double>(m, m->L[0], (const double*)m->p, eq, &m->sc->qp));
+      EpiPcgQ<double> eq{m->q, pd_out, m->L[0].mask};
+      FB_TRY(spmv_L<double>(m, m->L[0], (const double*)pd_out, eq, &m->sc->qp));
     }
     Level& L0 = m->L[0];
     const bool fs = fuse_s1(m);
@@ -1482,28 +1528,31 @@ static int body(fb_mg* m) {
   return FB_OK;
 }
 
-static int run_body(fb_mg* m) {
-  if (!m->cfg.use_graphs || debug_enabled()) return body(m);
+static int run_body(fb_mg* m, int j) {
+  if (!m->cfg.use_graphs || debug_enabled()) return body(m, j);
+  // one graph per parity of j (the direction buffers alternate)
+  const int par = j & 1;
   const int key = ((m->cfg.cycle * 4 + m->cfg.adapt_cgc) * 16 + m->cfg.flags) * 256 + m->cfg.format * 64 +
                   m->cfg.precision * 16 + m->cfg.outer * 4 + m->cfg.coarse;
-  if (!m->g_body || m->g_body_key != key) {
-    if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; }
+  cudaGraphExec_t& gb = m->g_body[par];
+  if (!gb || m->g_body_key[par] != key) {
+    if (gb) { cudaGraphExecDestroy(gb); gb = nullptr; }
     cudaGraph_t g = nullptr;
     FB_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
     const int before = m->launches;
-    int st = body(m);
+    int st = body(m, j);
     cudaError_t e = cudaStreamEndCapture(m->stream, &g);
     m->body_launches = m->launches - before;
     m->launches = before;
     if (st != FB_OK) { if (g) cudaGraphDestroy(g); return st; }
     if (e != cudaSuccess) return FB_ERR_CUDA;
-    e = cudaGraphInstantiate(&m->g_body, g, 0);
+    e = cudaGraphInstantiate(&gb, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { m->g_body = nullptr; return FB_ERR_CUDA; }
-    m->g_body_key = key;
+    if (e != cudaSuccess) { gb = nullptr; return FB_ERR_CUDA; }
+    m->g_body_key[par] = key;
   }
   m->launches += m->body_launches;
-  FB_CUDA(cudaGraphLaunch(m->g_body, m->stream));
+  FB_CUDA(cudaGraphLaunch(gb, m->stream));
   return FB_OK;
 }
 
@@ -1607,7 +1656,8 @@ static int ensure_vectors(fb_mg* m, int prec) {
   const uint32_t n = m->L[0].n;
   if (!m->r) {
     FB_TRY(dalloc(m, &m->r, n)); FB_TRY(dalloc(m, &m->p, n)); FB_TRY(dalloc(m, &m->q, n));
-    FB_TRY(dalloc(m, &m->p32, n));
+    FB_TRY(dalloc(m, &m->pb, n));
+    FB_TRY(dalloc(m, &m->p32, n)); FB_TRY(dalloc(m, &m->p32b, n));
     FB_TRY(dalloc(m, &m->xb, n)); FB_TRY(dalloc(m, &m->bb, n));
   }
   if (low && !m->r32) FB_TRY(dalloc(m, &m->r32, n));
@@ -1850,7 +1900,7 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
   // a staged kernel whose bounded wait expired has left rows unwritten: the solve stops at the
   // next read-back and returns FB_ERR_TIMEOUT (check_kernel_waits below)
   while (status == 1 && !host_kerr(m)) {
-    FB_TRY(run_body(m));
+    FB_TRY(run_body(m, it + 1));
     FB_CUDA(cudaStreamSynchronize(s));
     ++it;
     d = std::sqrt(*m->host_rr);
@@ -1858,8 +1908,12 @@ int solve_dev(fb_mg* m, const double* rhs, double* sol, double* hist, fb_solve_i
     status = st.analyse(it, d);
   }
   if (m->cfg.outer == FB_OUTER_PCG) {
-    if (pcg_p32(m)) k_pcg_finish<float><<<ew_grid(n), 256, 0, s>>>(m->xb, m->p32, m->sc, n);
-    else k_pcg_finish<double><<<ew_grid(n), 256, 0, s>>>(m->xb, m->p, m->sc, n);
+    // after `it` iterations: p_it is in buffer it & 1; an even count also holds alpha_{it-1} p_{it-1}
+    const bool odd = (it & 1) != 0;
+    if (pcg_p32(m))
+      k_pcg_finish2<float><<<ew_grid(n), 256, 0, s>>>(m->xb, m->p32b, odd ? m->p32b : m->p32, m->sc, n, odd ? 0 : 1);
+    else
+      k_pcg_finish2<double><<<ew_grid(n), 256, 0, s>>>(m->xb, m->pb, odd ? m->pb : m->p, m->sc, n, odd ? 0 : 1);
     m->launches++;
     FB_CHECK_LAUNCH();
   }
@@ -1917,7 +1971,8 @@ int fb_mg_configure(fb_mg* m, const fb_solver_cfg* c) {
   if (c->format != FB_FORMAT_MATFREE) FB_TRY(ensure_assembled(m, true, c->format == FB_FORMAT_SELL));
   m->cfg = *c;
   m->configured = true;
-  if (m->g_body) { cudaGraphExecDestroy(m->g_body); m->g_body = nullptr; m->g_body_key = -1; }
+  for (int q = 0; q < 2; ++q)
+    if (m->g_body[q]) { cudaGraphExecDestroy(m->g_body[q]); m->g_body[q] = nullptr; m->g_body_key[q] = -1; }
   m->prec_built = -1;
   return ensure_vectors(m, c->precision);
 }
@@ -1970,7 +2025,8 @@ void fb_mg_destroy(fb_mg* m) {
   if (!m) return;
   cudaSetDevice(m->device);
   if (m->stream) cudaStreamSynchronize(m->stream);
-  if (m->g_body) cudaGraphExecDestroy(m->g_body);
+  for (int q = 0; q < 2; ++q)
+    if (m->g_body[q]) cudaGraphExecDestroy(m->g_body[q]);
   for (void* p : m->allocs) cudaFree(p);
   if (m->host_rr) cudaFreeHost(m->host_rr);
   if (m->ev0) cudaEventDestroy(m->ev0);
@@ -2089,7 +2145,7 @@ int fb_mg_time_spmv(fb_mg* m, int level, int which, int prec, int reps, double* 
       EpiPcgQ<double> e{m->q, m->p, L.mask};
       return spmv_L<double>(m, L, (const double*)m->p, e, &m->sc->tmp[0]);
     }
-    if (which == 3) return pcgq_p32(m, &m->sc->tmp[0]);
+    if (which == 3) return pcgq_p32(m, &m->sc->tmp[0], m->p32);
     float* b = level == 0 ? m->r32 : L.rhs32;
     if (which == 0) { EpiJacobi<float, false> e{L.x32, b, L.invd32, L.y32, nullptr, L.mask, nullptr, float(m->cfg.omega_rich)}; return spmv_L<float>(m, L, L.x32, e, nullptr); }
     EpiDefect<float, false, false> e{L.def32, b, L.mask, nullptr};

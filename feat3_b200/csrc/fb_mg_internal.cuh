@@ -18,6 +18,8 @@ struct DevScalars {
   double qp;            // q . p
   double alpha;         // PCG step length whose x update is still pending (applied with the next
                         // direction update, or after the last iteration); 0 = none
+  double alpha_hold;    // the step length held over by an even iteration's direction update (its
+                        // x update is applied, before alpha's, by the next odd one); 0 = none
   double lvl[2 * kMaxLevels];  // [2l] ||rhs_l||^2, [2l+1] ||post-smoothing defect_l||^2
   double tmp[8];
   unsigned inject;      // test hook of the staged matrix-free kernel (fb_mg_test_expire_wait)
@@ -138,6 +140,8 @@ struct fb_mg {
   // outer (finest) vectors
   double *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *xb = nullptr, *bb = nullptr;
   float* p32 = nullptr;          // FP32 search direction of the mixed matrix-free form
+  double* pb = nullptr;          // second direction buffer: iteration j writes p_j into buffer j & 1
+  float* p32b = nullptr;         // (p / p32 for even j, pb / p32b for odd j)
   float* r32 = nullptr;
   // scalars / reduction workspace
   fb::DevScalars* sc = nullptr;
@@ -146,8 +150,8 @@ struct fb_mg {
   double* host_rr = nullptr;     // pinned
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // graphs
-  cudaGraphExec_t g_body = nullptr;
-  int g_body_key = -1;
+  cudaGraphExec_t g_body[2] = {nullptr, nullptr};  // the iteration body for odd and even iterations
+  int g_body_key[2] = {-1, -1};
   int launches = 0;
   int body_launches = 0;
   bool top_s1 = false;                   // finest-level first smoothing step already formed (fused)

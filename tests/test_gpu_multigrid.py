@@ -339,3 +339,28 @@ def test_stencil_stream_matches_packed(prec):
     assert s1["status"] == s2["status"] == "success" and s1["iters"] == s2["iters"]
     assert relerr(s1["u"].cpu().numpy(), s2["u"].cpu().numpy()) <= 1e-12
     mg.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_pcg_deferred_x_updates_match_the_defect(prec):
+    """PCG defers x += alpha p over two iterations (held in even iterations, applied in odd ones,
+    the rest after the last): stopped after every count of 1 to 5 iterations, the returned
+    iterate's true defect ||filter(b - A u)|| equals the defect the iteration carried (||r||),
+    so no pending step is lost or applied twice at either parity"""
+    import scipy.sparse as sp
+    from feat3_b200.solver import MultiGrid
+    lvl = 5
+    k = lognormal_k(3, lvl, 1.0, seed=29)
+    mg = MultiGrid.structured(3, 1, lvl, 1, k)
+    b = mg.assemble_rhs("one")
+    rp, ci, va = mg.export_csr(0)
+    A = sp.csr_matrix((va, ci, rp), shape=(len(rp) - 1, len(rp) - 1))
+    bc = po.Hierarchy(3, 1, lvl, lvl).filter()
+    bh = b.cpu().numpy()
+    for its in range(1, 6):
+        out = mg.configure(nu=2, precision=prec, format="matfree", tol=1e-30, max_iter=its).solve(b)
+        assert out["iters"] == its
+        r = bh - A @ out["u"].cpu().numpy()
+        r[bc] = 0.0
+        assert abs(np.linalg.norm(r) - out["def_final"]) <= 1e-11 * np.linalg.norm(bh), (its, np.linalg.norm(r), out["def_final"])
+    mg.close()
