@@ -82,8 +82,9 @@ static void debug_check_ptrs(const char* what, std::initializer_list<const void*
 
 template<typename VT, typename XT, typename AT, typename Epi>
 static int launch_sell(fb_mg* m, const DevSell& A, int prec, const XT* x, const Epi& epi, double* red_out) {
-  // 2-byte values: 16 slots in flight per lane (603 against 624 us per FP16 Jacobi step at 257^3)
-  auto fn = k_sell<VT, XT, AT, Epi, sizeof(VT) == 2 ? 16 : 8>;
+  // 2-byte values: 32 slots in flight per lane (578 against 602 us with 16 and 624 us with 8 per
+  // FP16 Jacobi step at 257^3)
+  auto fn = k_sell<VT, XT, AT, Epi, sizeof(VT) == 2 ? 32 : 8>;
   const int grid = occupancy_grid((const void*)fn, A.nchunks);
   if (debug_enabled())
     debug_check_ptrs("k_sell", {A.cs, A.cl, A.col, A.view(prec).val, (const void*)x, (const void*)m->ws,

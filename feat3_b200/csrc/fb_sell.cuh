@@ -346,21 +346,25 @@ __global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __r
 // W = 8 / sizeof(value) consecutive slots of its row: val[((c*G + g)*32 + lane)*W + e] holds
 // slot j = g*W + e (G = ceil(S/W); slots j >= S hold 0). A warp load is 256 contiguous bytes.
 template<typename VT> struct Pack8;
+// raw(): the 8 bytes as loaded; cvt(): their values as FP32 (ld = cvt(raw))
 template<> struct Pack8<__half> {
   static constexpr int W = 4;
-  __device__ __forceinline__ static void ld(const __half* p, float* v) {
-    const uint2 w = __ldcs(reinterpret_cast<const uint2*>(p));
+  __device__ __forceinline__ static uint2 raw(const __half* p) { return __ldcs(reinterpret_cast<const uint2*>(p)); }
+  __device__ __forceinline__ static void cvt(uint2 w, float* v) {
     const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&w.x));
     const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&w.y));
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
   }
+  __device__ __forceinline__ static void ld(const __half* p, float* v) { cvt(raw(p), v); }
 };
 template<> struct Pack8<float> {
   static constexpr int W = 2;
-  __device__ __forceinline__ static void ld(const float* p, float* v) {
-    const float2 w = __ldcs(reinterpret_cast<const float2*>(p));
-    v[0] = w.x; v[1] = w.y;
+  __device__ __forceinline__ static uint2 raw(const float* p) { return __ldcs(reinterpret_cast<const uint2*>(p)); }
+  __device__ __forceinline__ static void cvt(uint2 w, float* v) {
+    v[0] = __uint_as_float(w.x);
+    v[1] = __uint_as_float(w.y);
   }
+  __device__ __forceinline__ static void ld(const float* p, float* v) { cvt(raw(p), v); }
 };
 
 // slot j's neighbour offset on a lattice of CM1 points per side (slot j = (dz+1)*9 + (dy+1)*3 +

@@ -8,9 +8,9 @@
 // copied once per run with cp.async.bulk into an NST-deep mbarrier ring) and every consumer
 // thread walks up its column with a sliding 3x3x3 register window of x, so a row costs 9 shared
 // loads of the new line plus its own 8-byte stencil-value loads from global memory (coalesced
-// across the warp's consecutive rows). The 27 products are summed in slot order, as in
-// k_stencil_packed, so the rows' products and epilogues are bit-identical with it (the
-// reductions group their partial sums differently). The rows outside the slabs' interiors all
+// across the warp's consecutive rows, issued one row ahead). The 27 products are summed in slot
+// order, as in k_stencil_packed, so the rows' products and epilogues are bit-identical with it
+// (the reductions group their partial sums differently). The rows outside the slabs' interiors all
 // lie on the lattice boundary and are filtered: their epilogues run without the product.
 #pragma once
 #include "fb_mf_stream.cuh"
@@ -160,9 +160,26 @@ __global__ void __launch_bounds__(32 * (NCW + 1), 1)
         } else {
           const uint64_t r0 = (uint64_t(Z) * M1 + stp.y) * M1;
           const float* ss = reinterpret_cast<const float*>(st + off_s + grp * G.cap_s) + (r0 & (E - 1)) + X;
+          // the packed values of row r: 8-byte loads g = 0..NG-1 at vrow(r) + g * 32 * PW; each row's
+          // loads are issued one row ahead, so two rows' loads are in flight per thread
+          auto vrow = [&](uint32_t r) { return val + (size_t(r >> 5) * NG * 32 + (r & 31)) * PW; };
+          uint2 nraw[NG];
+          {
+            const VT* vp = vrow(uint32_t(r0) + X);
+#pragma unroll
+            for (int g = 0; g < NG; ++g) nraw[g] = Pack8<VT>::raw(vp + g * 32 * PW);
+          }
 #pragma unroll
           for (int j = 0; j < TY; ++j) {
             if (uint32_t(j) >= stp.nl) break;
+            uint2 craw[NG];
+#pragma unroll
+            for (int g = 0; g < NG; ++g) craw[g] = nraw[g];
+            if (j + 1 < TY && uint32_t(j + 1) < stp.nl) {
+              const VT* vq = vrow(uint32_t(r0) + uint32_t(j + 1) * M1 + X);
+#pragma unroll
+              for (int g = 0; g < NG; ++g) nraw[g] = Pack8<VT>::raw(vq + g * 32 * PW);
+            }
             // x lines y+j-1, y+j, y+j+1 are slots a, b, c
             const int a = j % 3, b = (j + 1) % 3, c = (j + 2) % 3;
 #pragma unroll
@@ -170,12 +187,11 @@ __global__ void __launch_bounds__(32 * (NCW + 1), 1)
 #pragma unroll
               for (int d = 0; d < 3; ++d) xw[q][c][d] = xs[q][j * int(M1) + d - 1];
             const uint32_t row = uint32_t(r0) + uint32_t(j) * M1 + X;
-            const VT* vp = val + (size_t(row >> 5) * NG * 32 + (row & 31)) * PW;
             float sum = 0.0f;
 #pragma unroll
             for (int g = 0; g < NG; ++g) {
               float v[PW];
-              Pack8<VT>::ld(vp + g * 32 * PW, v);
+              Pack8<VT>::cvt(craw[g], v);
 #pragma unroll
               for (int e = 0; e < PW; ++e) {
                 const int k = g * PW + e;  // slot k = (dz+1)*9 + (dy+1)*3 + (dx+1)
