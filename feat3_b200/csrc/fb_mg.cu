@@ -82,9 +82,11 @@ static void debug_check_ptrs(const char* what, std::initializer_list<const void*
 
 template<typename VT, typename XT, typename AT, typename Epi>
 static int launch_sell(fb_mg* m, const DevSell& A, int prec, const XT* x, const Epi& epi, double* red_out) {
-  // 2-byte values: 32 slots in flight per lane (578 against 602 us with 16 and 624 us with 8 per
-  // FP16 Jacobi step at 257^3)
-  auto fn = k_sell<VT, XT, AT, Epi, sizeof(VT) == 2 ? 32 : 8>;
+  // 2-byte values are read two slots per load from their interleaved layout (k_quant16_sell): 534
+  // against 579 us per FP16 Jacobi step at 257^3 with one 2-byte load per slot and 32 slots in
+  // flight per lane (602 us with 16, 624 us with 8); unrolling the pair loop 2 or 4 times ran 814-817
+  // us. Their odd last slot, if any, takes the slot loop below the pair loop.
+  auto fn = k_sell<VT, XT, AT, Epi, 8>;
   const int grid = occupancy_grid((const void*)fn, A.nchunks);
   if (debug_enabled())
     debug_check_ptrs("k_sell", {A.cs, A.cl, A.col, A.view(prec).val, (const void*)x, (const void*)m->ws,
@@ -561,9 +563,19 @@ __global__ void k_absmax(const double* __restrict__ v, uint64_t n, unsigned long
   if ((threadIdx.x & 31) == 0) atomicMax(out, __double_as_longlong(m));  // non-negative doubles order as integers
 }
 
-__global__ void k_quant16(__half* d, const double* __restrict__ s, double inv, uint64_t n) {
-  for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
-    d[i] = __double2half(s[i] * inv);
+// the SELL form's FP16 values: slot pairs of every chunk interleaved (k_sell's FP16 layout), one
+// warp per chunk
+__global__ void k_quant16_sell(__half* d, const double* __restrict__ s, double inv, const uint32_t* __restrict__ cs,
+                               const uint32_t* __restrict__ cl, uint32_t nchunks) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < nchunks; c += (gridDim.x * blockDim.x) >> 5) {
+    const uint32_t beg = cs[c], len = cl[c], even = len & ~1u;
+    for (uint32_t j = 0; j < len; ++j) {
+      const uint32_t src = beg + j * 32u + lane;
+      const uint32_t dst = j < even ? beg + (j >> 1) * 64u + 2u * lane + (j & 1u) : src;
+      d[dst] = __double2half(s[src] * inv);
+    }
+  }
 }
 
 unsigned ew_grid(uint64_t n) {
@@ -1634,7 +1646,8 @@ static int ensure_vectors(fb_mg* m, int prec) {
         const double scale = amax > 0.0 ? amax / 16384.0 : 1.0;
         L.A.scale16 = float(scale);
         FB_TRY(dalloc(m, &L.A.v16, L.A.nent));
-        k_quant16<<<ew_grid(L.A.nent), 256, 0, m->stream>>>(L.A.v16, L.A.v64, 1.0 / double(L.A.scale16), L.A.nent);
+        k_quant16_sell<<<ew_grid(uint64_t(L.A.nchunks) * 32), 256, 0, m->stream>>>(
+            L.A.v16, L.A.v64, 1.0 / double(L.A.scale16), L.A.cs, L.A.cl, L.A.nchunks);
         FB_CHECK_LAUNCH();
       }
     }

@@ -38,13 +38,19 @@ __device__ __forceinline__ float ld_stream(const __half* p) {
   return __half2float(__ushort_as_half(u));
 }
 
+// FP16 values of two slots per 4-byte load (the FP16 storage interleaves each chunk's slot pairs)
+__device__ __forceinline__ float2 ld_stream_pair(const __half* p) {
+  const unsigned u = __ldcs(reinterpret_cast<const unsigned*>(p));
+  return __half22float2(*reinterpret_cast<const __half2*>(&u));
+}
+
 struct SellView {
   uint32_t nchunks;
   uint32_t rows;
   const uint32_t* cs;    // nchunks+1 chunk starts (entries)
   const uint32_t* cl;    // nchunks chunk lengths (slots)
   const uint32_t* col;   // column per entry
-  const void* val;       // values (double / float / __half)
+  const void* val;       // values (double / float / __half; FP16: slot pairs interleaved, see k_sell)
   const uint32_t* perm;  // slot row -> matrix row (nullptr = identity)
   float scale;           // FP16 storage: a_ij = scale * h_ij (1 otherwise)
 };
@@ -201,6 +207,18 @@ __global__ void __launch_bounds__(256) k_sell(SellView A, const XT* __restrict__
     const uint32_t len = __ldg(A.cl + c);
     AT sum = AT(0);
     uint32_t j = 0;
+    if constexpr (sizeof(VT) == 2) {
+      // FP16: slots 2p and 2p+1 of a chunk are stored interleaved (entry cs + 64p + 2 lane + (j & 1)),
+      // so one 4-byte load per lane brings both values; an odd last slot keeps the plain layout.
+      // The products are summed in slot order, as in the plain form.
+      const VT* vpair = val + (beg - lane) + 2u * lane;
+      for (; j + 2 <= len; j += 2) {
+        const uint32_t c0 = ld_stream(A.col + beg + j * 32u), c1 = ld_stream(A.col + beg + (j + 1) * 32u);
+        const float2 v = ld_stream_pair(vpair + j * 32u);
+        sum += AT(v.x) * AT(__ldg(x + c0));
+        sum += AT(v.y) * AT(__ldg(x + c1));
+      }
+    }
     for (; j + UNROLL <= len; j += UNROLL) {
       uint32_t cc[UNROLL];
       AT vv[UNROLL];
