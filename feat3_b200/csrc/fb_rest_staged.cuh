@@ -124,6 +124,11 @@ __global__ void __launch_bounds__(288, 1) k_rest_q1_staged(MfTile G, uint32_t Mf
 #pragma unroll
           for (int c = 0; c < 3; ++c) v[a][0][c] = fp[a][c - 1];
         const uint32_t row0 = (g.Z * Mc1 + g.Y0 + l0) * Mc1 + Xc;
+        // the epilogue's inverse diagonal of the thread's rows, loaded together before the window
+        // (one at a time, each row's epilogue waited for its load)
+        T idv[TYC];
+#pragma unroll
+        for (int j = 0; j < TYC; ++j) idv[j] = (ei.sol1 && l0 + j < g.lt) ? __ldg(ei.invd + row0 + j * Mc1) : T(0);
 #pragma unroll
         for (int j = 0; j < TYC; ++j) {
           if (l0 + j >= g.lt) break;
@@ -143,7 +148,7 @@ __global__ void __launch_bounds__(288, 1) k_rest_q1_staged(MfTile G, uint32_t Mf
                 const T w = (b == 1 ? T(1) : T(0.5)) * (c == 1 ? T(1) : T(0.5)) * (a == 1 ? T(1) : T(0.5));
                 s += w * v[a][b][c];
               }
-          acc += ei(row0 + j * Mc1, s);
+          acc += ei.with_invd(row0 + j * Mc1, s, idv[j]);
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll

@@ -167,6 +167,14 @@ struct EpiRestrict {
     if (sol1) sol1[row] = m ? T(0) : omega * (id * v);
     return double(v) * double(v);
   }
+  // the same with the row's inverse diagonal already loaded (id; any value when sol1 is null)
+  __device__ __forceinline__ double with_invd(uint32_t row, T s, T id) const {
+    const bool m = masked(mask, row);
+    const T v = m ? T(0) : s;
+    rhs[row] = v;
+    if (sol1) sol1[row] = m ? T(0) : omega * (id * v);
+    return double(v) * double(v);
+  }
 };
 
 // prolongation + coarse-grid correction: sol += 1 * filter_cor(P sol_c)
@@ -177,6 +185,77 @@ struct EpiProlong {
   __device__ __forceinline__ double operator()(uint32_t row, T s) const {
     if (!masked(mask, row)) sol[row] = T(1) * s + sol[row];
     return 0.0;
+  }
+};
+
+// ------------------------------------------------------------------ epilogue operands ahead
+// The row inputs of an epilogue, loaded before the row's products are formed (at the start of
+// its chunk), so that their latency overlaps the products' loads instead of following them; the
+// arithmetic is the epilogue's own. Epilogues without a specialisation load nothing ahead, and
+// neither do the kernels that measured slower with it: the FP64 and FP32 SELL steps (926 -> 991
+// and 652 -> 659 us per Jacobi step at 257^3) and the FP64 stencil Jacobi step (647 -> 656 us,
+// EpiPreIf<false, ...>). Measured faster: the FP32 packed stencil step 365 -> 349 us, the FP64
+// stencil PCG-q 656 -> 639 us, the FP16 SELL step 527 -> 520 us.
+template<typename Epi>
+struct EpiPreNone {
+  struct type {};
+  __device__ __forceinline__ static type load(const Epi&, uint32_t) { return {}; }
+  template<typename S>
+  __device__ __forceinline__ static double apply(const Epi& e, uint32_t row, S s, const type&) {
+    return e(row, s);
+  }
+};
+template<typename Epi> struct EpiPre : EpiPreNone<Epi> {};
+template<bool ON, typename Epi> using EpiPreIf = typename std::conditional<ON, EpiPre<Epi>, EpiPreNone<Epi>>::type;
+
+template<typename T, bool RED, bool DOT>
+struct EpiPre<EpiJacobi<T, RED, DOT>> {
+  using E = EpiJacobi<T, RED, DOT>;
+  struct type { T b, id, xr; bool m; };
+  __device__ __forceinline__ static type load(const E& e, uint32_t row) {
+    return {e.rhs[row], e.invd ? e.invd[row] : T(0), e.x ? e.x[row] : T(0), masked(e.mask, row)};
+  }
+  __device__ __forceinline__ static double apply(const E& e, uint32_t row, T s, const type& p) {
+    if (smoother_skip<T>(e.skip_src)) {
+      const T o = e.s0 ? e.s0[row] : T(0);
+      e.out[row] = o;
+      return DOT ? double(o) * double(p.b) : 0.0;
+    }
+    const T d = p.b - s;
+    if (p.m) {
+      e.out[row] = p.xr;
+      return DOT ? double(p.xr) * double(p.b) : 0.0;
+    }
+    const T t = p.id * d;
+    const T o = e.omega * t + p.xr;
+    e.out[row] = o;
+    return RED ? double(d) * double(d) : (DOT ? double(o) * double(p.b) : 0.0);
+  }
+};
+
+template<typename T, bool RED, bool LOW>
+struct EpiPre<EpiDefect<T, RED, LOW>> {
+  using E = EpiDefect<T, RED, LOW>;
+  struct type { T b; bool m; };
+  __device__ __forceinline__ static type load(const E& e, uint32_t row) { return {e.rhs[row], masked(e.mask, row)}; }
+  __device__ __forceinline__ static double apply(const E& e, uint32_t row, T s, const type& p) {
+    T d = p.b - s;
+    if (p.m) d = T(0);
+    e.def[row] = d;
+    if (LOW) e.def32[row] = float(d);
+    return RED ? double(d) * double(d) : 0.0;
+  }
+};
+
+template<typename T, typename PT>
+struct EpiPre<EpiPcgQ<T, PT>> {
+  using E = EpiPcgQ<T, PT>;
+  struct type { PT pr; bool m; };
+  __device__ __forceinline__ static type load(const E& e, uint32_t row) { return {__ldg(e.p + row), masked(e.mask, row)}; }
+  __device__ __forceinline__ static double apply(const E& e, uint32_t row, T s, const type& p) {
+    const T v = p.m ? T(0) : s;
+    e.q[row] = v;
+    return double(v) * double(p.pr);
   }
 };
 
@@ -210,7 +289,12 @@ __global__ void __launch_bounds__(256) k_sell(SellView A, const XT* __restrict__
     if constexpr (sizeof(VT) == 2) {
       // FP16: slots 2p and 2p+1 of a chunk are stored interleaved (entry cs + 64p + 2 lane + (j & 1)),
       // so one 4-byte load per lane brings both values; an odd last slot keeps the plain layout.
-      // The products are summed in slot order, as in the plain form.
+      // The products are summed in slot order, as in the plain form. The row and its epilogue
+      // operands are loaded ahead of the products (EpiPre).
+      const uint32_t srow = c * 32u + lane;
+      const bool has = srow < A.rows;
+      const uint32_t row = has ? (A.perm ? __ldg(A.perm + srow) : srow) : 0u;
+      const typename EpiPre<Epi>::type pre = has ? EpiPre<Epi>::load(epi, row) : typename EpiPre<Epi>::type{};
       const VT* vpair = val + (beg - lane) + 2u * lane;
       for (; j + 2 <= len; j += 2) {
         const uint32_t c0 = ld_stream(A.col + beg + j * 32u), c1 = ld_stream(A.col + beg + (j + 1) * 32u);
@@ -218,6 +302,26 @@ __global__ void __launch_bounds__(256) k_sell(SellView A, const XT* __restrict__
         sum += AT(v.x) * AT(__ldg(x + c0));
         sum += AT(v.y) * AT(__ldg(x + c1));
       }
+      for (; j + UNROLL <= len; j += UNROLL) {
+        uint32_t cc[UNROLL];
+        AT vv[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) {
+          cc[u] = ld_stream(A.col + beg + (j + u) * 32u);
+          vv[u] = AT(ld_stream(val + beg + (j + u) * 32u));
+        }
+#pragma unroll
+        for (int u = 0; u < UNROLL; ++u) sum += vv[u] * AT(__ldg(x + cc[u]));
+      }
+      for (; j < len; ++j) {
+        const uint32_t cc = ld_stream(A.col + beg + j * 32u);
+        sum += AT(ld_stream(val + beg + j * 32u)) * AT(__ldg(x + cc));
+      }
+      if (has) {
+        sum *= AT(A.scale);
+        acc += EpiPre<Epi>::apply(epi, row, sum, pre);
+      }
+      continue;
     }
     for (; j + UNROLL <= len; j += UNROLL) {
       uint32_t cc[UNROLL];
@@ -237,7 +341,6 @@ __global__ void __launch_bounds__(256) k_sell(SellView A, const XT* __restrict__
     const uint32_t srow = c * 32u + lane;
     if (srow < A.rows) {
       const uint32_t row = A.perm ? __ldg(A.perm + srow) : srow;
-      if (sizeof(VT) == 2) sum *= AT(A.scale);
       acc += epi(row, sum);
     }
   }
@@ -314,6 +417,8 @@ __global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __r
     const int32_t row0 = int32_t(c) * 32;
     const int32_t row = row0 + lane;
     const VT* vp = val + size_t(c) * S * 32 + lane;
+    using Pre = EpiPreIf<std::is_same<Epi, EpiPcgQ<AT, XT>>::value, Epi>;
+    const typename Pre::type pre = row <= last ? Pre::load(epi, uint32_t(row)) : typename Pre::type{};
     // warp-uniform: every neighbour of every row of the chunk lies inside the vector
     const bool inside = row0 + A.off[0] >= 0 && row0 + 31 + A.off[S - 1] <= last;
     AT sum = AT(0);
@@ -351,7 +456,7 @@ __global__ void __launch_bounds__(256) k_stencil(StencilView<S> A, const XT* __r
     }
     if (row <= last) {
       if (sizeof(VT) == 2) sum *= AT(A.scale);
-      acc += epi(uint32_t(row), sum);
+      acc += Pre::apply(epi, uint32_t(row), sum, pre);
     }
   }
   if (Epi::kReduce) {
@@ -414,6 +519,8 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
     const int32_t row0 = int32_t(c) * 32;
     const int32_t row = row0 + lane;
     const VT* vp = val + (size_t(c) * G * 32 + lane) * W;
+    const typename EpiPre<Epi>::type pre =
+        row <= last ? EpiPre<Epi>::load(epi, uint32_t(row)) : typename EpiPre<Epi>::type{};
     const bool inside = row0 + off(0) >= 0 && row0 + 31 + off(S - 1) <= last;
     float sum = 0.0f;
     if (inside) {
@@ -444,7 +551,7 @@ __global__ void __launch_bounds__(256, 4) k_stencil_packed(StencilView<S> A, con
     }
     if (row <= last) {
       if (sizeof(VT) == 2) sum *= A.scale;
-      acc += epi(uint32_t(row), sum);
+      acc += EpiPre<Epi>::apply(epi, uint32_t(row), sum, pre);
     }
   }
   if (Epi::kReduce) {
