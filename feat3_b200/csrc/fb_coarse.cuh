@@ -143,24 +143,34 @@ __device__ __forceinline__ T coarse_prol(const CLevel<T>& F, const CLevel<T>& C,
   return s;
 }
 
-// one Jacobi step at row i from the product s (EpiJacobi without skip)
+// a row's smoothing inputs (its x, rhs and inverse diagonal values and its filter bit), loaded
+// before the row's product so that they do not wait behind its gathers
 template<typename T>
-__device__ __forceinline__ T jacobi_row(const CLevel<T>& L, T om, const T* cur, const T* b, uint32_t i, T s) {
-  const T xc = ldc(cur + i);
-  const T d = ldc(b + i) - s;
-  return masked(L.mask, i) ? xc : om * (__ldg(L.invd + i) * d) + xc;
+struct RowIn {
+  T xc, b, id;
+  bool m;
+};
+template<typename T>
+__device__ __forceinline__ RowIn<T> row_in(const CLevel<T>& L, const T* cur, const T* b, uint32_t i) {
+  return {ldc(cur + i), ldc(b + i), __ldg(L.invd + i), masked(L.mask, i)};
 }
 
-// post-smoothing step at row i (EpiJacobi with s0 and skip test; the first step reduces ||d||^2)
+// one Jacobi step at a row from the product s (EpiJacobi without skip)
 template<typename T>
-__device__ __forceinline__ T post_row(const CLevel<T>& L, T om, const T* cur, const T* b, const T* s0, uint32_t i, T s,
-                                      bool skip, bool first, double& acc) {
-  if (skip) return ldc(s0 + i);
-  const T xc = ldc(cur + i);
-  const T d = ldc(b + i) - s;
-  if (masked(L.mask, i)) return xc;
+__device__ __forceinline__ T jacobi_row(T om, const RowIn<T>& in, T s) {
+  const T d = in.b - s;
+  return in.m ? in.xc : om * (in.id * d) + in.xc;
+}
+
+// post-smoothing step at a row (EpiJacobi with s0 = o0 and skip test; the first step reduces
+// ||d||^2)
+template<typename T>
+__device__ __forceinline__ T post_row(T om, const RowIn<T>& in, T o0, T s, bool skip, bool first, double& acc) {
+  if (skip) return o0;
+  const T d = in.b - s;
+  if (in.m) return in.xc;
   if (first) acc += double(d) * double(d);
-  return om * (__ldg(L.invd + i) * d) + xc;
+  return om * (in.id * d) + in.xc;
 }
 
 // deterministic cluster-wide sum; ends with a cluster barrier, result in every thread. Each CTA
@@ -212,16 +222,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
     }
     for (int it = 1; it < nu; ++it) {
       for (uint32_t i = gt; i < L.n; i += gs) {
+        const RowIn<T> in = row_in(L, cur, b, i);  // ahead of the row's gathers
         const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
-        oth[i] = skip ? T(0) : jacobi_row(L, om, cur, b, i, s);
+        oth[i] = skip ? T(0) : jacobi_row(om, in, s);
       }
       cl.sync();
       T* tmp = cur; cur = oth; oth = tmp;
     }
     sol[l] = cur;
     for (uint32_t i = gt; i < L.n; i += gs) {
+      const T bi = ldc(b + i);
+      const bool mk = masked(L.mask, i);
       const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
-      L.def[i] = masked(L.mask, i) ? T(0) : ldc(b + i) - s;
+      L.def[i] = mk ? T(0) : bi - s;
     }
     cl.sync();
     const CLevel<T>& C = A.L[l + 1];
@@ -301,8 +314,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
       const double dv = sqrt(dn);
       const bool skip = it > 0 && (!isfinite(dv) || dv <= double(eps_of<T>()) * double(eps_of<T>()));
       for (uint32_t i = gt; i < L.n; i += gs) {
+        const RowIn<T> in = row_in(L, cur, b, i);  // ahead of the row's gathers
+        const T o0 = skip ? ldc(s0 + i) : T(0);
         const T s = coarse_row<T, DIM>(L, cur, int32_t(i));
-        oth[i] = post_row(L, om, cur, b, s0, i, s, skip, it == 0, acc);
+        oth[i] = post_row(om, in, o0, s, skip, it == 0, acc);
       }
       if (it == 0) {
         dn = cluster_sum<THREADS>(acc, part[rk++ & 1], sh, cl);
