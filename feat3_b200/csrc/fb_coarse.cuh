@@ -242,9 +242,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
     double acc = 0.0;
     for (uint32_t i = gt; i < C.n; i += gs) {
       const bool mk = masked(C.mask, i);
+      const T id = s1 ? __ldg(C.invd + i) : T(0);  // ahead of the restriction's loads
       const T v = mk ? T(0) : coarse_rest<T, DIM>(L, C, L.def, i);
       C.rhs[i] = v;
-      if (s1) C.x[i] = mk ? T(0) : om * (__ldg(C.invd + i) * v);
+      if (s1) C.x[i] = mk ? T(0) : om * (id * v);
       acc += double(v) * double(v);
     }
     bnorm = cluster_sum<THREADS>(acc, part[rk++ & 1], sh, cl);
@@ -304,8 +305,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_coarse_cycle(CoarseArgs<T> A) {
     const T* b = L.rhs;
     T* cur = sol[l];
     T* oth = (cur == L.x) ? L.y : L.x;
-    for (uint32_t i = gt; i < L.n; i += gs)
-      if (!masked(L.mask, i)) cur[i] = T(1) * coarse_prol<T, DIM>(L, C, sol[l + 1], i) + ldc(cur + i);
+    for (uint32_t i = gt; i < L.n; i += gs) {
+      if (masked(L.mask, i)) continue;
+      const T xo = ldc(cur + i);  // ahead of the prolongation's loads
+      cur[i] = T(1) * coarse_prol<T, DIM>(L, C, sol[l + 1], i) + xo;
+    }
     cl.sync();
     T* s0 = cur;
     double dn = 0.0;
