@@ -86,23 +86,30 @@ def coefficient(level, seed):
 
 # ------------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 50 ms while the headline form runs: start()
+    returns once the sampler has printed its first line (at most 5 s), and only the samples read
+    after that point count, so they all fall in the form's warm-up and timed solves."""
     def __init__(self, index):
-        self.index, self.samples, self.proc = index, [], None
+        self.index, self.samples, self.proc, self.t_begin = index, [], None, 0.0
 
     def start(self):
         q = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
+        self.t_begin = time.time()
 
     def _read(self):
         for line in self.proc.stdout:
-            self.samples.append([s.strip() for s in line.split(",")])
+            self.samples.append((time.time(), [s.strip() for s in line.split(",")]))
 
     def stop(self):
         if not self.proc:
@@ -112,12 +119,13 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm = [float(s[0]) for s in self.samples if len(s) >= 8 and s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if len(s) >= 8 and s[1].replace(".", "").isdigit()]
+        run = [f for t, f in self.samples if t >= self.t_begin]
+        sm = [float(s[0]) for s in run if len(s) >= 8 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in run if len(s) >= 8 and s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples if len(s) >= 8 for i in range(4) if s[4 + i] == "Active"})
+        reasons = sorted({names[i] for s in run if len(s) >= 8 for i in range(4) if s[4 + i] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(run)}
 
 
 # ------------------------------------------------------------------------------- CPU reference
